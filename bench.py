@@ -1,0 +1,399 @@
+"""Benchmark: Darcy head solves/s at 256^3 (||b - A h|| / ||b|| <= 1e-10) + face velocity.
+
+Workload (default): 256 x 256 x 256 cells, lnK Gaussian with variance 4, exponential
+covariance, correlation length 8 cells, randomization method with 1000 modes (seeded
+synthetic field, no dataset), h = 1 at x = 0, h = 0 at x = L, no-flow elsewhere.  One step
+= set-up from K (coarsening, face coefficients, RHS) + PCG to 1e-10 + face velocities, K
+resident in HBM.  Every array is larger than L2 (126 MB), so no flush is needed.
+
+Arms:
+  default           this library (mixed precision: FP32 V-cycle in flexible FP64 PCG), with
+                    the plain FP64 CCMG-PCG of this library measured beside it;
+  --impl reference  the reference's own solve_head (PCG_MG) + compute_velocity_from_head,
+                    compiled from its sources into oracle/_ref, on the same K and tolerance.
+Multi-GPU (torchrun): independent replicas, one realisation per rank, no collective on the
+data path ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            self.f.flush()
+            for line in open(self.f.name):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        finally:
+            os.unlink(self.f.name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_K(M, n, sigma2, lam, seed, device):
+    import torch
+    g = M.Grid3D(n, n, n, 1.0)
+    with torch.cuda.device(device):
+        return M.generate_K_field(g, sigma2, (lam, lam, lam), seed=seed, n_modes=1000)
+
+
+def levels_for(n):
+    lv, m = 1, n
+    while m > 4 and m % 2 == 0:
+        m //= 2
+        lv += 1
+    return lv
+
+
+def solver_cfg(M, n, precision, rtol=1e-10):
+    return M.HeadSolveConfig(mg_levels=levels_for(n), mg_pre_smooth=2, mg_post_smooth=2,
+                             mg_coarse_iters=50, cg_max_iter=500, cg_check_every=1, cg_rtol=rtol,
+                             conv_norm=M.CONV_B, precision=precision)
+
+
+def run_steps(M, n, K, precision, steps, warmup, dist_ctx=None):
+    """Times `steps` device-resident steps; returns dict with per-step ms and last result."""
+    import torch
+    g = M.Grid3D(n, n, n, 1.0)
+    bc = M.BCSpec.darcy_x()
+    stream = torch.cuda.current_stream()
+    s = M.HeadSolver(g, bc, solver_cfg(M, n, precision), stream=stream.cuda_stream)
+    h = torch.empty_like(K)
+    su, sv, sw = M.velocity_sizes(g)
+    U = torch.empty(su, dtype=torch.float64, device=K.device)
+    V = torch.empty(sv, dtype=torch.float64, device=K.device)
+    W = torch.empty(sw, dtype=torch.float64, device=K.device)
+
+    def step():
+        s.set_K(K)
+        r = s.solve(h)
+        M.compute_velocity_from_head(U, V, W, h, K, g, bc)
+        return r
+
+    res = None
+    for _ in range(warmup):
+        res = step()
+    if dist_ctx is not None:
+        dist_ctx.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    iters = []
+    for _ in range(steps):
+        res = step()
+        iters.append(res.num_iterations)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist_ctx is not None:
+        dist_ctx.barrier()
+    ms = e0.elapsed_time(e1)
+    return dict(solver=s, ms_total=ms, res=res, iters=iters, h=h, launches=s.setup_launches + res.kernel_launches + 1)
+
+
+def e2e_steps(M, n, K_host, precision, steps, warmup):
+    """Same metric through the public API with HOST buffers: H2D of K from pinned memory,
+    set-up + solve + velocity, D2H of the head, every step."""
+    import torch
+    g = M.Grid3D(n, n, n, 1.0)
+    bc = M.BCSpec.darcy_x()
+    stream = torch.cuda.current_stream()
+    s = M.HeadSolver(g, bc, solver_cfg(M, n, precision), stream=stream.cuda_stream)
+    Kd = torch.empty(K_host.shape, dtype=torch.float64, device="cuda")
+    h = torch.empty_like(Kd)
+    h_host = torch.empty(K_host.shape, dtype=torch.float64, pin_memory=True)
+    su, sv, sw = M.velocity_sizes(g)
+    U = torch.empty(su, dtype=torch.float64, device="cuda")
+    V = torch.empty(sv, dtype=torch.float64, device="cuda")
+    W = torch.empty(sw, dtype=torch.float64, device="cuda")
+
+    def step():
+        Kd.copy_(K_host, non_blocking=True)
+        s.set_K(Kd)
+        s.solve(h)
+        M.compute_velocity_from_head(U, V, W, h, Kd, g, bc)
+        h_host.copy_(h, non_blocking=True)
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    nbytes = K_host.numel() * 8
+    s.close()
+    return steps / (ms / 1e3), nbytes, nbytes
+
+
+def cpu_baseline(K_np, n, iters_needed, budget_s=20.0):
+    """The oracle (OpenMP restatement of the reference CCMG-PCG) on all host cores, on a
+    bounded sample: set-up + 1 and + 3 PCG iterations of the same solve, extrapolated to the
+    iteration count the same algorithm needs (taken from this library's FP64 solve)."""
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    bc = O.baseline_bc()
+    lv = levels_for(n)
+    t = time.perf_counter()
+    O.solve_head_pcg(K_np, bc, lv, max_iter=1, check_every=1, rtol=1e-30)
+    t1 = time.perf_counter() - t
+    per_iter = None
+    if t1 < budget_s / 3:
+        t = time.perf_counter()
+        O.solve_head_pcg(K_np, bc, lv, max_iter=3, check_every=1, rtol=1e-30)
+        t3 = time.perf_counter() - t
+        per_iter = max((t3 - t1) / 2, 1e-9)
+    else:
+        per_iter = t1 / 2  # set-up ~ one iteration; crude bound when the budget is exhausted
+    setup = max(t1 - per_iter, 0.0)
+    total = setup + per_iter * iters_needed
+    # velocity: one pass over h, K (timed on the same data)
+    t = time.perf_counter()
+    O.velocity(K_np, K_np, bc)
+    total += time.perf_counter() - t
+    return {"value": 1.0 / total, "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": f"oracle PCG set-up + 1 and + 3 iterations at {n}^3, extrapolated to "
+                      f"{iters_needed} iterations (+ one velocity pass); {total:.1f} s per solve"}
+
+
+def roofline(prof, hbm, src):
+    """Dominant kernel by time per PCG iteration; achieved = algorithmic bytes / launch time."""
+    best = None
+    for name, ms, nbytes, per_iter in prof:
+        if nbytes <= 0 or per_iter <= 0:
+            continue
+        tot = ms * per_iter
+        if best is None or tot > best[0]:
+            best = (tot, name, ms, nbytes)
+    if best is None:
+        return None
+    _, name, ms, nbytes = best
+    ach = nbytes / (ms * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get(name)
+    return {"kernel": name, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+            "frac": round(ach / hbm, 4), "peak_source": src, "traffic": traffic,
+            "alg_bytes_per_launch": nbytes, "ms_per_launch": round(ms, 5)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32", "bf16"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-kernels", action="store_true", help="print per-kernel timings")
+    ap.add_argument("--seed", type=int, default=20240601)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist_ctx = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        dist_ctx = dist
+    else:
+        torch.cuda.set_device(0)
+    n = args.size
+    sigma2, lam = 4.0, 8.0
+    config = {"workload": f"darcy_ccmg_pcg_{n}^3_sigma2_{sigma2:g}_lambda_{lam:g}",
+              "grid": [n, n, n], "cells": n ** 3, "lnK": "gaussian, exponential covariance, 1000 modes",
+              "tolerance": "||b-Ah||/||b|| <= 1e-10", "bc": "h=1 at x=0, h=0 at x=L, no-flow elsewhere",
+              "step": "set-up from K + PCG + face velocity", "l2": "inputs larger than L2 (no flush)",
+              "parallelism": f"replicas{world}" if world > 1 else "single"}
+    hbm, src = peaks()
+
+    if args.impl == "reference":
+        if rank != 0:
+            if dist_ctx is not None:
+                dist_ctx.destroy_process_group()
+            return
+        print(json.dumps(reference_arm(args, n, sigma2, lam, config)), flush=True)
+        if dist_ctx is not None:
+            dist_ctx.destroy_process_group()
+        return
+
+    import macroflow3d_b200 as M
+    from macroflow3d_b200 import build
+    build.build_lib()
+    prec = {"fp64": M.PREC_FP64, "fp32": M.PREC_FP32, "bf16": M.PREC_BF16}[args.precision]
+    K = make_K(M, n, sigma2, lam, args.seed + rank, torch.cuda.current_device())
+    torch.cuda.synchronize()
+
+    with Clocks(torch.cuda.current_device()) as clk:
+        out = run_steps(M, n, K, prec, args.steps, args.warmup, dist_ctx)
+    clocks = clk.summary()
+    ms = out["ms_total"]
+    if dist_ctx is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist_ctx.all_reduce(t, op=dist_ctx.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * args.steps / (ms / 1e3)
+    res = out["res"]
+    line = {"metric": "darcy_solves_per_s_256cubed_relres_1e-10", "value": round(value, 4),
+            "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 outer / f32 V-cycle" if prec == M.PREC_FP32 else args.precision,
+            "data": "synthetic (seeded randomization-method lnK field)", "config": config}
+    line["iterations"] = out["iters"][-1]
+    line["true_rel_residual"] = res.true_rel_residual
+    line["cell_updates_per_s"] = round(n ** 3 * out["iters"][-1] * value / world * world, 1)
+    line["gpu_launches"] = out["launches"] * args.steps
+    line["clocks"] = clocks
+
+    if rank == 0:
+        prof = out["solver"].profile(reps=10)
+        line["roofline"] = roofline(prof, hbm, src)
+        if args.profile_kernels:
+            line["kernels"] = [{"name": a, "ms": round(b, 5), "GBps": round(c / (b * 1e-3) / 1e9, 1) if b > 0 else None,
+                                "per_iter": d} for a, b, c, d in prof]
+    out["solver"].close()
+
+    if not args.no_fp64_compare and prec != M.PREC_FP64:
+        o64 = run_steps(M, n, K, M.PREC_FP64, args.steps, args.warmup, dist_ctx)
+        ms64 = o64["ms_total"]
+        line["fp64_plain"] = {"solves_per_s": round(world * args.steps / (ms64 / 1e3), 4),
+                              "iterations": o64["iters"][-1],
+                              "true_rel_residual": o64["res"].true_rel_residual}
+        d = (out["h"] - o64["h"]).abs().max().item() / o64["h"].abs().max().item()
+        line["head_rel_maxdiff_vs_fp64"] = d
+        line["speedup_vs_fp64_plain"] = round(value / line["fp64_plain"]["solves_per_s"], 3)
+        iters64 = o64["iters"][-1]
+        o64["solver"].close()
+    else:
+        iters64 = out["iters"][-1]
+
+    if rank == 0 and world == 1 and not args.no_e2e:
+        K_host = K.cpu().pin_memory()
+        v, bi, bo = e2e_steps(M, n, K_host, prec, max(2, args.steps // 2), 1)
+        line["e2e"] = {"value": round(v, 4), "unit": "solves/s", "h2d_bytes_per_step": bi,
+                       "d2h_bytes_per_step": bo}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(K.cpu().numpy(), n, iters64)
+
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist_ctx is not None:
+        dist_ctx.barrier()
+        dist_ctx.destroy_process_group()
+
+
+def reference_arm(args, n, sigma2, lam, config):
+    """The reference's stock solve_head(PCG_MG) + compute_velocity_from_head, from oracle/_ref."""
+    import numpy as np
+    import torch
+    from oracle import oracle as O
+    import macroflow3d_b200 as M
+    base = {"impl": "reference", "metric": "darcy_solves_per_s_256cubed_relres_1e-10", "unit": "solves/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded randomization-method lnK field)", "config": config}
+    K = make_K(M, n, sigma2, lam, args.seed, 0).cpu().numpy()
+    bc = O.baseline_bc()
+    O.set_threads(os.cpu_count() or 1)
+    b = O.build_rhs(K, bc)
+    r0 = np.linalg.norm(b - O.apply_A(K, O.init_guess(K.shape, bc), bc))
+    rtol = 1e-10 * np.linalg.norm(b) / r0  # the reference tests ||r||/||r0||; ask for ||r||/||b||
+    if O.ref_available():
+        ms, it, conv, _, _, _ = O.ref_bench(K, bc, levels_for(n), 500, 1, rtol, args.warmup, args.steps)
+        total = float(np.sum(ms))
+        value = args.steps / (total / 1e3)
+        base.update({"value": round(value, 4), "ms_per_step": round(total / args.steps, 3),
+                     "iterations": it, "converged": conv,
+                     "cpu_baseline": {"value": round(value, 4), "unit": "solves/s", "cores": 0,
+                                      "kind": "reference",
+                                      "sample": "the reference's CUDA solve_head + velocity (built from its "
+                                                "sources into oracle/_ref), full solves on one B200"},
+                     "e2e": {"value": round(value, 4), "unit": "solves/s", "h2d_bytes_per_step": 0,
+                             "d2h_bytes_per_step": 0}})
+        return base
+    # the reference was not built: the oracle port on the host cores
+    cb = cpu_baseline(K, n, 30)
+    base.update({"value": cb["value"], "ms_per_step": 1e3 / cb["value"], "cpu_baseline": cb,
+                 "e2e": {"value": cb["value"], "unit": "solves/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0}})
+    return base
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,206 @@
+/*
+ * mf3d.h -- C-ABI of the B200-native Darcy head solve + face velocity (libmf3d.so).
+ *
+ * Drop-in boundary for MacroFlow3D's head-solver path.  Each entry point names the
+ * reference routine it replaces (paths within santi-esquerre/MacroFlow3D).  Conventions:
+ *   - plain C types only; device pointers are `double*` (or `void*` where the precision
+ *     varies), streams are `void*` holding a cudaStream_t (NULL = the solver's own stream
+ *     for solver calls, the legacy default stream otherwise);
+ *   - every call returns an int status: 0 ok, < 0 error (see MF3D_E_*); the message of the
+ *     last error on the calling thread is returned by mf3d_last_error();
+ *   - arrays are cell-centred, x fastest: cell (i,j,k) at i + nx*(j + ny*k)
+ *     (src/core/Grid3D.hpp:54);
+ *   - no exceptions cross the ABI; non-convergence is reported in the result struct, as in
+ *     the reference (src/physics/flow/solve_head.cuh:136-141), not as an error.
+ */
+#ifndef MF3D_H
+#define MF3D_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------------- */
+#define MF3D_OK 0
+#define MF3D_E_INVALID (-1)   /* bad argument / unsupported configuration */
+#define MF3D_E_CUDA (-2)      /* CUDA runtime error */
+#define MF3D_E_NOMEM (-3)     /* device allocation failed */
+#define MF3D_E_STATE (-4)     /* call out of order (e.g. solve before set_K) */
+
+/* ---- BCType, src/core/BCSpec.hpp:13 ------------------------------------------------------ */
+#define MF3D_BC_DIRICHLET 0
+#define MF3D_BC_NEUMANN 1
+#define MF3D_BC_PERIODIC 2
+
+/* ---- HeadSolverType, src/physics/flow/solve_head.cuh:52-56 -------------------------------- */
+#define MF3D_SOLVER_PCG_MG 0
+#define MF3D_SOLVER_MG 1
+#define MF3D_SOLVER_CG 2
+
+/* ---- PinMode, src/numerics/pin_spec.hpp:56-60 --------------------------------------------- */
+#define MF3D_PIN_AUTO 0
+#define MF3D_PIN_ON 1
+#define MF3D_PIN_OFF 2
+
+/* ---- V-cycle precision (extension: the reference is FP64 only) ---------------------------- */
+#define MF3D_PREC_FP64 0 /* FP64 V-cycle, FP64 face coefficients */
+#define MF3D_PREC_FP32 1 /* FP32 V-cycle, FP32 face coefficients, FP64 coarse tail */
+#define MF3D_PREC_BF16 2 /* FP32 V-cycle, BF16 face coefficients with per-level 2^s scale */
+
+/* ---- stopping-test denominator ------------------------------------------------------------ */
+#define MF3D_CONV_R0 0 /* ||r|| / ||r0|| < cg_rtol, as src/numerics/solvers/pcg.cuh:156-164 */
+#define MF3D_CONV_B 1  /* ||r|| / ||b||  < cg_rtol */
+
+/* ---- velocity layouts, src/physics/common/fields.cuh:230 ---------------------------------- */
+#define MF3D_VEL_COMPACT 0 /* U (nx+1)*ny*nz, V nx*(ny+1)*nz, W nx*ny*(nz+1) */
+#define MF3D_VEL_PADDED 1  /* (nx+1)*(ny+1)*(nz+1) per component, padded_layout.cuh:30 */
+
+/* Grid3D (src/core/Grid3D.hpp:32-55); isotropic spacing, as every reference kernel assumes. */
+typedef struct mf3d_grid {
+    int nx, ny, nz;
+    double dx;
+} mf3d_grid;
+
+/* BCSpec / BCSpecDevice (src/core/BCSpec.hpp:36-88, BCSpecDevice.cuh:12-51):
+ * faces in the order xmin, xmax, ymin, ymax, zmin, zmax. */
+typedef struct mf3d_bc {
+    int type[6];
+    double value[6];
+} mf3d_bc;
+
+/* HeadSolveConfig (src/physics/flow/solve_head.cuh:63-96) plus this library's extensions. */
+typedef struct mf3d_solver_config {
+    int solver;          /* MF3D_SOLVER_* (default PCG_MG) */
+    int mg_levels;       /* maximum number of levels (default 4) */
+    int mg_pre_smooth;   /* GSRB sweeps before restriction (default 2) */
+    int mg_post_smooth;  /* GSRB sweeps after prolongation (default 2) */
+    int mg_max_cycles;   /* standalone MG: maximum V-cycles (default 20) */
+    int mg_coarse_iters; /* GSRB sweeps on the coarsest level (default 50) */
+    int cg_max_iter;     /* default 1000 */
+    int cg_check_every;  /* default 10 */
+    double cg_rtol;      /* default 1e-8 */
+    double rtol;         /* standalone MG tolerance (default 1e-6) */
+    int pin_mode;        /* MF3D_PIN_* (default AUTO) */
+    /* extensions */
+    int precision;       /* MF3D_PREC_* (default FP64) */
+    int flexible;        /* -1 auto (Polak-Ribiere beta when precision != FP64), 0 FR, 1 PR */
+    int conv_norm;       /* MF3D_CONV_* (default R0, the reference's test) */
+    int use_graph;       /* 1 (default): whole PCG loop in one CUDA graph (device while loop) */
+} mf3d_solver_config;
+
+/* HeadSolveResult (src/physics/flow/solve_head.cuh:136-141) plus diagnostics. */
+typedef struct mf3d_solve_result {
+    int num_iterations;
+    int converged;
+    int status;              /* 0 ok, 1 breakdown (pAp = 0), 2 non-finite, 3 device-time budget exceeded */
+    int num_levels;
+    double initial_residual; /* ||r0|| */
+    double final_residual;   /* ||r|| at the last check (recurrence residual) */
+    double true_rel_residual;/* ||b - A h|| / ||b|| recomputed after the loop */
+    double b_norm;           /* ||b|| */
+    float device_ms;         /* device time of set-up-free solve (CUDA events) */
+    int kernel_launches;     /* kernels this library launched for the solve */
+} mf3d_solve_result;
+
+/* Per-kernel timing record (diagnostics; no counterpart in the reference). */
+typedef struct mf3d_kernel_timing {
+    char name[40];
+    float ms;              /* mean device time per launch (CUDA events, launch stream) */
+    double bytes;          /* algorithmic bytes per launch (each input read once, output written once) */
+    int launches_per_iter; /* launches of this kernel per PCG iteration */
+} mf3d_kernel_timing;
+
+typedef struct mf3d_head_solver mf3d_head_solver;
+
+/* Library / error handling ------------------------------------------------------------------ */
+const char* mf3d_last_error(void);
+const char* mf3d_version(void);
+
+/* HeadSolveConfig defaults (solve_head.cuh:63-96; pin auto). */
+int mf3d_default_config(mf3d_solver_config* cfg);
+
+/* Head solver: owns the multigrid hierarchy, face coefficients, PCG workspace and CUDA
+ * graph.  Replaces FlowWorkspace + the set-up part of solve_head
+ * (src/physics/common/workspaces.cuh:111-167, src/physics/flow/solve_head.cu:89-125). */
+int mf3d_head_solver_create(const mf3d_grid* grid, const mf3d_bc* bc, const mf3d_solver_config* cfg,
+                            void* stream, mf3d_head_solver** out);
+int mf3d_head_solver_destroy(mf3d_head_solver* s);
+int mf3d_head_solver_num_levels(const mf3d_head_solver* s);
+/* Bytes of device memory the solver holds. */
+long long mf3d_head_solver_device_bytes(const mf3d_head_solver* s);
+
+/* Conductivity set-up: copies K (device, FP64, n cells), coarsens it to every level
+ * (coarsen_K, src/physics/flow/coarsen_K.cu:55-77), builds every level's face coefficients,
+ * the right-hand side (build_rhs_head, rhs_head.cu:121-194) and the initial guess
+ * (init_head_guess, solve_head.cu:56-73). */
+int mf3d_head_solver_set_K(mf3d_head_solver* s, const double* K_dev);
+
+/* solve_head(h, K, grid, bc, cfg, ctx, ws) (src/physics/flow/solve_head.cuh:158-160).
+ * h_dev: output head (device, n).  x0_dev: initial guess (device) or NULL for the
+ * reference's x-linear guess.  Blocks until the result is known. */
+int mf3d_head_solve(mf3d_head_solver* s, double* h_dev, const double* x0_dev, mf3d_solve_result* res);
+
+/* MultigridPreconditioner::apply (src/numerics/solvers/mg_preconditioner.cu:16-44):
+ * z = one V-cycle on r from a zero guess, with the solver's hierarchy (after set_K).
+ * r_dev, z_dev: FP64 device arrays of n cells. */
+int mf3d_head_solver_vcycle(mf3d_head_solver* s, const double* r_dev, double* z_dev);
+
+/* Diagnostics (no counterpart in the reference): times, with CUDA events on the solver's
+ * stream, `reps` launches of each kernel of one PCG iteration on the current state (call after
+ * a solve; the solver state is scratch afterwards and is rebuilt by the next solve).  Fills
+ * up to `cap` records and sets *count. */
+int mf3d_head_solver_profile(mf3d_head_solver* s, int reps, mf3d_kernel_timing* out, int cap, int* count);
+/* Kernels launched by the last mf3d_head_solver_set_K (diagnostics). */
+int mf3d_head_solver_setup_launches(const mf3d_head_solver* s);
+
+/* compute_velocity_from_head (src/physics/flow/velocity_from_head.cuh:54-73): Darcy face
+ * velocities, layout MF3D_VEL_*.  Padded entries that are not faces are left untouched. */
+int mf3d_velocity_from_head(const mf3d_grid* grid, const mf3d_bc* bc, const double* h_dev,
+                            const double* K_dev, int layout, double* U_dev, double* V_dev, double* W_dev,
+                            void* stream);
+
+/* Velocity (compact layout) plus discrete mass balance, fused: out_host[0] = max over cells
+ * of |sum_f q_f A_f|, out_host[1] = Q_in through x = 0, out_host[2] = Q_out through x = L.
+ * (verify_mean_velocity_darcy, velocity_from_head.cu:964, has no caller in the reference.) */
+int mf3d_velocity_mass_balance(const mf3d_grid* grid, const mf3d_bc* bc, const double* h_dev,
+                               const double* K_dev, double* U_dev, double* V_dev, double* W_dev,
+                               double* out_host, void* stream);
+
+/* ---- operator pieces (device pointers, FP64; in-place where the reference is) ------------- */
+/* VarCoeffLaplacian::apply, src/numerics/operators/varcoeff_laplacian.cu:241-277 */
+int mf3d_apply_A(const mf3d_grid* g, const mf3d_bc* bc, int pin, const double* K, const double* x,
+                 double* y, void* stream);
+/* gsrb_smooth_3d, src/multigrid/smoothers/gsrb_3d.cu:368-576 (x updated in place) */
+int mf3d_gsrb(const mf3d_grid* g, const mf3d_bc* bc, int pin, const double* K, const double* b,
+              double* x, int iters, void* stream);
+/* compute_residual_3d, src/multigrid/smoothers/residual_3d.cu:378-502 */
+int mf3d_residual(const mf3d_grid* g, const mf3d_bc* bc, int pin, const double* K, const double* x,
+                  const double* b, double* r, void* stream);
+/* restrict_3d, src/multigrid/transfer/restrict_3d.cu:55-80 (coarse = fine / 2) */
+int mf3d_restrict(const mf3d_grid* coarse, const double* r_fine, double* b_coarse, void* stream);
+/* prolong_3d_add, src/multigrid/transfer/prolong_3d.cu:520-621 */
+int mf3d_prolong_add(const mf3d_grid* coarse, const double* x_coarse, double* x_fine, void* stream);
+/* coarsen_K, src/physics/flow/coarsen_K.cu:55-77 */
+int mf3d_coarsen_K(const mf3d_grid* coarse, const double* K_fine, double* K_coarse, void* stream);
+/* build_rhs_head, src/physics/flow/rhs_head.cu:121-194 */
+int mf3d_build_rhs(const mf3d_grid* g, const mf3d_bc* bc, const double* K, double* b, void* stream);
+/* init_head_guess, src/physics/flow/solve_head.cu:56-73 */
+int mf3d_init_head_guess(const mf3d_grid* g, const mf3d_bc* bc, double* h, void* stream);
+
+/* ---- K-field generator (randomization method; generate_K_field, src/physics/stochastic/
+ * stochastic.cu:270-367, with per-axis correlation lengths added) ------------------------- */
+#define MF3D_COV_EXPONENTIAL 0
+#define MF3D_COV_GAUSSIAN 1
+/* Host-side mode sampling (no GPU): modes_host receives 5*n_modes doubles laid out as
+ * k1[n], k2[n], k3[n], a[n], b[n]; counter-based (Philox4x32-10) stream from `seed`. */
+int mf3d_kfield_modes(unsigned long long seed, int n_modes, int covariance, double lambda_x,
+                      double lambda_y, double lambda_z, double* modes_host);
+/* K (or lnK when want_exp = 0) at the cell centres of g from device-resident modes. */
+int mf3d_kfield_eval(const mf3d_grid* g, int n_modes, const double* modes_dev, double sigma2,
+                     double log_kg, int want_exp, double* out_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MF3D_H */

@@ -1,0 +1,303 @@
+"""macroflow3d_b200 -- B200-native Darcy head solve (CCMG-preconditioned CG) and face velocity.
+
+Python mirror of the reference's head-solver interface (santi-esquerre/MacroFlow3D:
+solve_head, init_head_guess, build_rhs_head, coarsen_K, compute_velocity_from_head, the
+multigrid free functions and VarCoeffLaplacian::apply) over the C-ABI of libmf3d.so.
+Device arrays are torch CUDA tensors (float64, contiguous, numel = nx*ny*nz in the
+reference's i + nx*(j + ny*k) layout); torch provides memory and the current stream only.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional, Tuple
+
+from . import _lib
+from ._lib import Mf3dError, check, lib
+from .config import (BCFace, BCSpec, ConfigError, FlowConfig, load_flow_yaml, parse_flow,  # noqa: F401
+                     DIRICHLET, NEUMANN, PERIODIC, PIN_AUTO, PIN_OFF, PIN_ON)
+
+SOLVER_PCG_MG, SOLVER_MG, SOLVER_CG = 0, 1, 2
+PREC_FP64, PREC_FP32, PREC_BF16 = 0, 1, 2
+CONV_R0, CONV_B = 0, 1
+VEL_COMPACT, VEL_PADDED = 0, 1
+COV_EXPONENTIAL, COV_GAUSSIAN = 0, 1
+
+
+@dataclass
+class Grid3D:
+    """Grid3D (src/core/Grid3D.hpp:32-55): isotropic spacing dx."""
+    nx: int
+    ny: int
+    nz: int
+    dx: float = 1.0
+
+    def num_cells(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    def c(self) -> _lib.Grid:
+        return _lib.Grid(self.nx, self.ny, self.nz, float(self.dx))
+
+
+def _bc(bc: BCSpec) -> _lib.BC:
+    out = _lib.BC()
+    for f in range(6):
+        out.type[f] = int(bc.faces[f].type)
+        out.value[f] = float(bc.faces[f].value)
+    return out
+
+
+@dataclass
+class HeadSolveConfig:
+    """HeadSolveConfig (src/physics/flow/solve_head.cuh:63-96) + extensions."""
+    solver_type: int = SOLVER_PCG_MG
+    mg_levels: int = 4
+    mg_pre_smooth: int = 2
+    mg_post_smooth: int = 2
+    mg_max_cycles: int = 20
+    mg_coarse_iters: int = 50
+    cg_max_iter: int = 1000
+    cg_check_every: int = 10
+    cg_rtol: float = 1e-8
+    rtol: float = 1e-6
+    pin_mode: int = PIN_AUTO
+    precision: int = PREC_FP64
+    flexible: int = -1
+    conv_norm: int = CONV_R0
+    use_graph: int = 1
+
+    @staticmethod
+    def from_yaml(flow: FlowConfig) -> "HeadSolveConfig":
+        """HeadSolveConfig::from_yaml (solve_head.cuh:98-130)."""
+        st = {"cg": SOLVER_CG, "mg": SOLVER_MG}.get(flow.solver, SOLVER_PCG_MG)
+        flex = {"auto": -1, True: 1, False: 0, "true": 1, "false": 0}.get(flow.flexible, -1)
+        return HeadSolveConfig(st, flow.mg_levels, flow.mg_pre_smooth, flow.mg_post_smooth,
+                               flow.mg_max_cycles, flow.mg_coarse_iters, flow.cg_max_iter,
+                               flow.cg_check_every, flow.cg_rtol, flow.rtol, flow.pin_mode,
+                               {"fp64": 0, "fp32": 1, "bf16": 2}[str(flow.precision)], flex,
+                               CONV_B if flow.conv_norm == "b" else CONV_R0, int(bool(flow.use_graph)))
+
+    def c(self) -> _lib.SolverConfig:
+        return _lib.SolverConfig(self.solver_type, self.mg_levels, self.mg_pre_smooth,
+                                 self.mg_post_smooth, self.mg_max_cycles, self.mg_coarse_iters,
+                                 self.cg_max_iter, self.cg_check_every, float(self.cg_rtol),
+                                 float(self.rtol), self.pin_mode, self.precision, self.flexible,
+                                 self.conv_norm, self.use_graph)
+
+
+@dataclass
+class HeadSolveResult:
+    """HeadSolveResult (solve_head.cuh:136-141) + diagnostics."""
+    num_iterations: int
+    initial_residual: float
+    final_residual: float
+    converged: bool
+    status: int
+    num_levels: int
+    true_rel_residual: float
+    b_norm: float
+    device_ms: float
+    kernel_launches: int = 0
+
+
+def _ptr(t) -> int:
+    import torch
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("tensor must be contiguous")
+    return t.data_ptr()
+
+
+def _f64(t, n: int, name: str):
+    import torch
+    if t.dtype != torch.float64:
+        raise TypeError(f"{name} must be float64")
+    if t.numel() < n:
+        raise ValueError(f"{name} buffer too small")
+    return _ptr(t)
+
+
+def _stream():
+    import torch
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class HeadSolver:
+    """Owns the hierarchy, face coefficients, PCG workspace and CUDA graph of one grid
+    (the reference's FlowWorkspace, src/physics/common/workspaces.cuh:111-167)."""
+
+    def __init__(self, grid: Grid3D, bc: BCSpec, cfg: Optional[HeadSolveConfig] = None,
+                 stream=None):
+        self.grid, self.bc = grid, bc
+        self.cfg = cfg or HeadSolveConfig()
+        h = C.c_void_p()
+        s = C.c_void_p(stream) if isinstance(stream, int) else (stream or C.c_void_p())
+        check(lib().mf3d_head_solver_create(C.byref(grid.c()), C.byref(_bc(bc)),
+                                            C.byref(self.cfg.c()), s, C.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().mf3d_head_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def num_levels(self) -> int:
+        return lib().mf3d_head_solver_num_levels(self._h)
+
+    @property
+    def device_bytes(self) -> int:
+        return lib().mf3d_head_solver_device_bytes(self._h)
+
+    def set_K(self, K) -> None:
+        check(lib().mf3d_head_solver_set_K(self._h, _f64(K, self.grid.num_cells(), "K")))
+
+    def solve(self, h, x0=None) -> HeadSolveResult:
+        n = self.grid.num_cells()
+        r = _lib.SolveResult()
+        check(lib().mf3d_head_solve(self._h, _f64(h, n, "h"),
+                                    None if x0 is None else _f64(x0, n, "x0"), C.byref(r)))
+        return HeadSolveResult(r.num_iterations, r.initial_residual, r.final_residual,
+                               bool(r.converged), r.status, r.num_levels, r.true_rel_residual,
+                               r.b_norm, r.device_ms, r.kernel_launches)
+
+    @property
+    def setup_launches(self) -> int:
+        return lib().mf3d_head_solver_setup_launches(self._h)
+
+    def profile(self, reps: int = 20):
+        """[(name, ms per launch, algorithmic bytes per launch, launches per iteration)] for
+        every kernel of one PCG iteration, timed with CUDA events (diagnostics)."""
+        cap = 64
+        arr = (_lib.KernelTiming * cap)()
+        cnt = C.c_int(0)
+        check(lib().mf3d_head_solver_profile(self._h, int(reps), arr, cap, C.byref(cnt)))
+        return [(arr[i].name.decode(), float(arr[i].ms), float(arr[i].bytes), int(arr[i].launches_per_iter))
+                for i in range(cnt.value)]
+
+    def vcycle(self, r, z) -> None:
+        """MultigridPreconditioner::apply (src/numerics/solvers/mg_preconditioner.cu:16-44)."""
+        n = self.grid.num_cells()
+        check(lib().mf3d_head_solver_vcycle(self._h, _f64(r, n, "r"), _f64(z, n, "z")))
+
+
+def solve_head(h, K, grid: Grid3D, bc: BCSpec, cfg: HeadSolveConfig,
+               workspace: Optional[HeadSolver] = None) -> Tuple[HeadSolveResult, HeadSolver]:
+    """solve_head (src/physics/flow/solve_head.cuh:158-160).  Returns (result, workspace);
+    pass the workspace back in to reuse the hierarchy and graph, as FlowWorkspace is reused."""
+    import torch
+    if workspace is None or workspace.grid != grid:
+        workspace = HeadSolver(grid, bc, cfg, stream=torch.cuda.current_stream().cuda_stream)
+    workspace.set_K(K)
+    return workspace.solve(h), workspace
+
+
+def init_head_guess(h, grid: Grid3D, bc: BCSpec) -> None:
+    check(lib().mf3d_init_head_guess(C.byref(grid.c()), C.byref(_bc(bc)),
+                                     _f64(h, grid.num_cells(), "h"), _stream()))
+
+
+def build_rhs_head(rhs, K, grid: Grid3D, bc: BCSpec) -> None:
+    n = grid.num_cells()
+    check(lib().mf3d_build_rhs(C.byref(grid.c()), C.byref(_bc(bc)), _f64(K, n, "K"),
+                               _f64(rhs, n, "rhs"), _stream()))
+
+
+def coarsen_K(coarse: Grid3D, K_fine, K_coarse) -> None:
+    n = coarse.num_cells()
+    check(lib().mf3d_coarsen_K(C.byref(coarse.c()), _f64(K_fine, 8 * n, "K_fine"),
+                               _f64(K_coarse, n, "K_coarse"), _stream()))
+
+
+def apply_A(grid: Grid3D, bc: BCSpec, K, x, y, pin: bool = False) -> None:
+    """VarCoeffLaplacian::apply (src/numerics/operators/varcoeff_laplacian.cu:241-277)."""
+    n = grid.num_cells()
+    check(lib().mf3d_apply_A(C.byref(grid.c()), C.byref(_bc(bc)), int(pin), _f64(K, n, "K"),
+                             _f64(x, n, "x"), _f64(y, n, "y"), _stream()))
+
+
+def gsrb_smooth_3d(grid: Grid3D, x, b, K, num_iters: int, bc: BCSpec, pin: bool = False) -> None:
+    """gsrb_smooth_3d (src/multigrid/smoothers/gsrb_3d.cu:368-576); x updated in place."""
+    n = grid.num_cells()
+    check(lib().mf3d_gsrb(C.byref(grid.c()), C.byref(_bc(bc)), int(pin), _f64(K, n, "K"),
+                          _f64(b, n, "b"), _f64(x, n, "x"), int(num_iters), _stream()))
+
+
+def compute_residual_3d(grid: Grid3D, x, b, K, r, bc: BCSpec, pin: bool = False) -> None:
+    """compute_residual_3d (src/multigrid/smoothers/residual_3d.cu:378-502)."""
+    n = grid.num_cells()
+    check(lib().mf3d_residual(C.byref(grid.c()), C.byref(_bc(bc)), int(pin), _f64(K, n, "K"),
+                              _f64(x, n, "x"), _f64(b, n, "b"), _f64(r, n, "r"), _stream()))
+
+
+def restrict_3d(coarse: Grid3D, r_fine, b_coarse) -> None:
+    n = coarse.num_cells()
+    check(lib().mf3d_restrict(C.byref(coarse.c()), _f64(r_fine, 8 * n, "r_fine"),
+                              _f64(b_coarse, n, "b_coarse"), _stream()))
+
+
+def prolong_3d_add(coarse: Grid3D, x_coarse, x_fine) -> None:
+    n = coarse.num_cells()
+    check(lib().mf3d_prolong_add(C.byref(coarse.c()), _f64(x_coarse, n, "x_coarse"),
+                                 _f64(x_fine, 8 * n, "x_fine"), _stream()))
+
+
+def velocity_sizes(grid: Grid3D, layout: int = VEL_COMPACT) -> Tuple[int, int, int]:
+    nx, ny, nz = grid.nx, grid.ny, grid.nz
+    if layout == VEL_PADDED:
+        s = (nx + 1) * (ny + 1) * (nz + 1)
+        return s, s, s
+    return (nx + 1) * ny * nz, nx * (ny + 1) * nz, nx * ny * (nz + 1)
+
+
+def compute_velocity_from_head(U, V, W, h, K, grid: Grid3D, bc: BCSpec,
+                               layout: int = VEL_COMPACT) -> None:
+    """compute_velocity_from_head (src/physics/flow/velocity_from_head.cuh:54-73)."""
+    n = grid.num_cells()
+    su, sv, sw = velocity_sizes(grid, layout)
+    check(lib().mf3d_velocity_from_head(C.byref(grid.c()), C.byref(_bc(bc)), _f64(h, n, "h"),
+                                        _f64(K, n, "K"), int(layout), _f64(U, su, "U"),
+                                        _f64(V, sv, "V"), _f64(W, sw, "W"), _stream()))
+
+
+def velocity_mass_balance(U, V, W, h, K, grid: Grid3D, bc: BCSpec) -> Tuple[float, float, float]:
+    """Compact velocity + (max_c |div_c|, Q_in, Q_out)."""
+    n = grid.num_cells()
+    su, sv, sw = velocity_sizes(grid, VEL_COMPACT)
+    out = (C.c_double * 3)()
+    check(lib().mf3d_velocity_mass_balance(C.byref(grid.c()), C.byref(_bc(bc)), _f64(h, n, "h"),
+                                           _f64(K, n, "K"), _f64(U, su, "U"), _f64(V, sv, "V"),
+                                           _f64(W, sw, "W"), out, _stream()))
+    return out[0], out[1], out[2]
+
+
+def kfield_modes(seed: int, n_modes: int = 1000, covariance: int = COV_EXPONENTIAL,
+                 lam=(1.0, 1.0, 1.0)):
+    """Randomization-method modes (host, no GPU): numpy array (5, n_modes) = k1,k2,k3,a,b."""
+    import numpy as np
+    out = np.empty(5 * n_modes, dtype=np.float64)
+    check(lib().mf3d_kfield_modes(int(seed), int(n_modes), int(covariance), float(lam[0]),
+                                  float(lam[1]), float(lam[2]),
+                                  out.ctypes.data_as(C.POINTER(C.c_double))))
+    return out.reshape(5, n_modes)
+
+
+def generate_K_field(grid: Grid3D, sigma2: float, lam=(1.0, 1.0, 1.0), seed: int = 0,
+                     n_modes: int = 1000, covariance: int = COV_EXPONENTIAL, K_geo: float = 1.0,
+                     log_only: bool = False):
+    """generate_K_field (src/physics/stochastic/stochastic.cu:270-367) with per-axis
+    correlation lengths: K = K_geo * exp(lnK) as a float64 CUDA tensor (nz, ny, nx)."""
+    import math
+    import torch
+    modes = torch.from_numpy(kfield_modes(seed, n_modes, covariance, lam)).cuda()
+    out = torch.empty((grid.nz, grid.ny, grid.nx), dtype=torch.float64, device="cuda")
+    check(lib().mf3d_kfield_eval(C.byref(grid.c()), int(n_modes), modes.data_ptr(), float(sigma2),
+                                 math.log(K_geo), 0 if log_only else 1, out.data_ptr(), _stream()))
+    return out

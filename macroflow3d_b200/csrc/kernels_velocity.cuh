@@ -1,0 +1,109 @@
+// kernels_velocity.cuh -- Darcy face velocities from head, and the discrete mass balance.
+//
+// One kernel writes all three components (the reference launches 3 interior + 6 boundary
+// kernels on the legacy default stream, src/physics/flow/velocity_from_head.cu:601-777).
+// Formulas are the reference's: interior q = -[2 K_L K_R / (K_L + K_R)] (h_R - h_L)/dx;
+// Dirichlet faces -K_c (h_c - h_bc)/(dx/2) (min side) and -K_c (h_bc - h_c)/(dx/2) (max side);
+// Neumann 0; periodic faces use the wrapped neighbour (velocity_from_head.cu:102-381).
+#pragma once
+#include "kernels_setup.cuh"
+#include "mf3d_device.cuh"
+
+namespace mf3d {
+
+__device__ __forceinline__ double hm_vel(double a, double b) { return 2.0 * a * b / (a + b); }
+
+struct VelOut {
+    double* U;
+    double* V;
+    double* W;
+    int layout; // 0 compact MAC, 1 padded (nx+1)(ny+1)(nz+1)
+};
+
+__device__ __forceinline__ size_t u_idx(int layout, int i, int j, int k, int nx, int ny) {
+    return layout ? (size_t)k * (ny + 1) * (nx + 1) + (size_t)j * (nx + 1) + i
+                  : (size_t)i + (size_t)j * (nx + 1) + (size_t)k * (nx + 1) * ny;
+}
+__device__ __forceinline__ size_t v_idx(int layout, int i, int j, int k, int nx, int ny) {
+    return layout ? (size_t)k * (ny + 1) * (nx + 1) + (size_t)j * (nx + 1) + i
+                  : (size_t)i + (size_t)j * nx + (size_t)k * nx * (ny + 1);
+}
+__device__ __forceinline__ size_t w_idx(int layout, int i, int j, int k, int nx, int ny) {
+    return layout ? (size_t)k * (ny + 1) * (nx + 1) + (size_t)j * (nx + 1) + i
+                  : (size_t)i + (size_t)j * nx + (size_t)k * nx * ny;
+}
+
+// Flux through the min-side face of cell c along one axis.  `lo` is 1 when the cell is on
+// the min boundary of that axis, cw the wrapped neighbour index for periodic, cn the
+// in-domain neighbour otherwise.
+__device__ __forceinline__ double face_min(const double* H, const double* K, size_t c, size_t cn, size_t cw,
+                                           bool lo, int type, double hbc, double d) {
+    if (!lo) return -hm_vel(K[cn], K[c]) * (H[c] - H[cn]) / d;
+    if (type == BC_DIRICHLET) return -K[c] * (H[c] - hbc) / (d * 0.5);
+    if (type == BC_PERIODIC) return -hm_vel(K[cw], K[c]) * (H[c] - H[cw]) / d;
+    return 0.0;
+}
+__device__ __forceinline__ double face_max_bnd(const double* H, const double* K, size_t c, size_t cw, int type,
+                                               double hbc, double d) {
+    if (type == BC_DIRICHLET) return -K[c] * (hbc - H[c]) / (d * 0.5);
+    if (type == BC_PERIODIC) return -hm_vel(K[c], K[cw]) * (H[cw] - H[c]) / d;
+    return 0.0;
+}
+
+constexpr int VEL_NT = 256;
+
+// Writes U,V,W.  With mb != null also accumulates the mass balance:
+// mb[0] = max_c |sum_f q_f A_f| (as ordered bits), mb[1] = Q_in (x=0), mb[2] = Q_out (x=L).
+__global__ void __launch_bounds__(VEL_NT) velocity_kernel(int nx, int ny, int nz, double dx,
+                                                          const double* __restrict__ H, const double* __restrict__ K,
+                                                          BcDev bc, VelOut o, unsigned long long* mb_max,
+                                                          double* partials, unsigned* ticket, double* mb_sums) {
+    const size_t n = (size_t)nx * ny * nz;
+    const size_t nxy = (size_t)nx * ny;
+    double qin = 0.0, qout = 0.0, mx = 0.0;
+    const double A = dx * dx;
+    for (size_t c = blockIdx.x * (size_t)VEL_NT + threadIdx.x; c < n; c += (size_t)gridDim.x * VEL_NT) {
+        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / nxy);
+        const double u0 = face_min(H, K, c, c - 1, c + (nx - 1), i == 0, bc.type[0], bc.value[0], dx);
+        const double v0 = face_min(H, K, c, c - nx, c + (size_t)(ny - 1) * nx, j == 0, bc.type[2], bc.value[2], dx);
+        const double w0 = face_min(H, K, c, c - nxy, c + (size_t)(nz - 1) * nxy, k == 0, bc.type[4], bc.value[4], dx);
+        o.U[u_idx(o.layout, i, j, k, nx, ny)] = u0;
+        o.V[v_idx(o.layout, i, j, k, nx, ny)] = v0;
+        o.W[w_idx(o.layout, i, j, k, nx, ny)] = w0;
+        // plus faces: the neighbour's min face, or the max boundary
+        double u1, v1, w1;
+        if (i < nx - 1) u1 = -hm_vel(K[c], K[c + 1]) * (H[c + 1] - H[c]) / dx;
+        else {
+            u1 = face_max_bnd(H, K, c, c - (nx - 1), bc.type[1], bc.value[1], dx);
+            o.U[u_idx(o.layout, nx, j, k, nx, ny)] = u1;
+        }
+        if (j < ny - 1) v1 = -hm_vel(K[c], K[c + nx]) * (H[c + nx] - H[c]) / dx;
+        else {
+            v1 = face_max_bnd(H, K, c, c - (size_t)(ny - 1) * nx, bc.type[3], bc.value[3], dx);
+            o.V[v_idx(o.layout, i, ny, k, nx, ny)] = v1;
+        }
+        if (k < nz - 1) w1 = -hm_vel(K[c], K[c + nxy]) * (H[c + nxy] - H[c]) / dx;
+        else {
+            w1 = face_max_bnd(H, K, c, c - (size_t)(nz - 1) * nxy, bc.type[5], bc.value[5], dx);
+            o.W[w_idx(o.layout, i, j, nz, nx, ny)] = w1;
+        }
+        if (mb_max) {
+            const double d = ((u1 - u0) + (v1 - v0) + (w1 - w0)) * A;
+            mx = fmax(mx, fabs(d));
+            if (i == 0) qin += u0 * A;
+            if (i == nx - 1) qout += u1 * A;
+        }
+    }
+    if (mb_max) {
+        double v[2] = {qin, qout}, out[2];
+        // max: non-negative doubles order like their bit patterns
+        for (int ofs = 16; ofs > 0; ofs >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, ofs));
+        if ((threadIdx.x & 31) == 0) atomicMax(mb_max, (unsigned long long)__double_as_longlong(mx));
+        if (grid_sums<VEL_NT, 2>(v, partials, ticket, gridDim.x, out)) {
+            mb_sums[0] = out[0];
+            mb_sums[1] = out[1];
+        }
+    }
+}
+
+} // namespace mf3d

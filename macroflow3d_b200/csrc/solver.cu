@@ -1,0 +1,1355 @@
+// solver.cu -- host orchestration behind the C-ABI in include/mf3d.h.
+//
+// HeadSolver replaces the reference's FlowWorkspace + solve_head (src/physics/flow/
+// solve_head.cu:75-243) for the PCG_MG path:
+//   set_K : coarsen K to every level, build face coefficients (FP64 for the fine operator and
+//           the coarse tail, FP32 / BF16 for a mixed-precision V-cycle), RHS, initial guess;
+//   solve : r0 = b - A x0, then the PCG loop as ONE CUDA graph whose `while` node body is
+//           [V-cycle -> z, <r,z>] [p = z + beta p] [Ap, <p,Ap>] [x, r update, stop test];
+//           the stop test sets the while condition on the device, so the host waits once.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../../include/mf3d.h"
+#include "kernels_kfield.cuh"
+#include "kernels_mg.cuh"
+#include "kernels_pcg.cuh"
+#include "kernels_setup.cuh"
+#include "kernels_velocity.cuh"
+
+namespace mf3d {
+
+static thread_local std::string g_err;
+
+// Device-time limit of one solve: the PCG loop stops with status 3 after this long.
+static constexpr unsigned long long kSolveBudgetNs = 120ull * 1000000000ull;
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define MF3D_CK(call)                                                                                   \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess)                                                                          \
+            throw Error(e_ == cudaErrorMemoryAllocation ? MF3D_E_NOMEM : MF3D_E_CUDA,                   \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                            \
+    } while (0)
+// every kernel launch goes through this check; the counter feeds the launch statistics
+static thread_local long long g_launches = 0;
+#define MF3D_LAUNCH_CK()                                                                                \
+    do {                                                                                                \
+        ++g_launches;                                                                                   \
+        MF3D_CK(cudaGetLastError());                                                                    \
+    } while (0)
+
+static int g_num_sms = 0;
+static int num_sms() {
+    if (g_num_sms == 0) {
+        int dev = 0;
+        MF3D_CK(cudaGetDevice(&dev));
+        MF3D_CK(cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    return g_num_sms;
+}
+
+static unsigned grid1d(size_t n, int nt, int per_sm = 8) {
+    const size_t want = (n + nt - 1) / nt;
+    const size_t cap = (size_t)num_sms() * per_sm;
+    return (unsigned)std::max<size_t>(1, std::min(want, cap));
+}
+
+// RAII device allocation
+struct DevMem {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevMem() = default;
+    explicit DevMem(size_t b) { alloc(b); }
+    void alloc(size_t b) {
+        release();
+        bytes = b;
+        if (b) MF3D_CK(cudaMalloc(&p, b));
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    ~DevMem() { release(); }
+    DevMem(const DevMem&) = delete;
+    DevMem& operator=(const DevMem&) = delete;
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+static BcDev to_dev(const mf3d_bc& bc) {
+    BcDev d;
+    for (int f = 0; f < 6; ++f) {
+        d.type[f] = bc.type[f];
+        d.value[f] = bc.value[f];
+    }
+    return d;
+}
+
+static void validate_bc(const mf3d_bc& bc) {
+    // BCSpec::validate, src/core/BCSpec.hpp:66-86
+    for (int a = 0; a < 3; ++a) {
+        const bool p0 = bc.type[2 * a] == MF3D_BC_PERIODIC, p1 = bc.type[2 * a + 1] == MF3D_BC_PERIODIC;
+        if (p0 != p1) throw Error(MF3D_E_INVALID, "Periodic BC must be specified on both faces of an axis");
+    }
+    for (int f = 0; f < 6; ++f) {
+        if (bc.type[f] < 0 || bc.type[f] > 2) throw Error(MF3D_E_INVALID, "unknown BC type");
+        if (!std::isfinite(bc.value[f])) throw Error(MF3D_E_INVALID, "BC values must be finite");
+    }
+}
+
+static bool has_dirichlet(const mf3d_bc& bc) {
+    for (int f = 0; f < 6; ++f)
+        if (bc.type[f] == MF3D_BC_DIRICHLET) return true;
+    return false;
+}
+
+// pin_enabled, src/numerics/pin_spec.hpp:109-120
+static bool pin_enabled(int mode, const mf3d_bc& bc) {
+    if (mode == MF3D_PIN_ON) return true;
+    if (mode == MF3D_PIN_OFF) return false;
+    return !has_dirichlet(bc);
+}
+
+struct Geom {
+    int nx, ny, nz;
+    size_t n;
+    double dx;
+};
+
+// Levels by halving every axis (MGHierarchy, src/multigrid/mg_types.hpp:86-99): at most
+// `max_levels`, stop when a coarse axis would be < 2.  An axis of odd length is never
+// halved (the reference's 2:1 restriction is undefined there), so coarsening also stops
+// at the first odd axis.
+static std::vector<Geom> make_levels(const mf3d_grid& g, int max_levels) {
+    std::vector<Geom> L;
+    Geom c{g.nx, g.ny, g.nz, (size_t)g.nx * g.ny * g.nz, g.dx};
+    for (int l = 0; l < std::max(1, max_levels); ++l) {
+        L.push_back(c);
+        if (l == max_levels - 1) break;
+        if ((c.nx & 1) || (c.ny & 1) || (c.nz & 1)) break;
+        Geom d{c.nx / 2, c.ny / 2, c.nz / 2, 0, c.dx * 2.0};
+        if (d.nx < 2 || d.ny < 2 || d.nz < 2) break;
+        d.n = (size_t)d.nx * d.ny * d.nz;
+        c = d;
+    }
+    return L;
+}
+
+template <class TC> static LevelOp<TC> make_op(const Geom& G, const mf3d_bc& bc, bool pin, double scale) {
+    LevelOp<TC> L{};
+    L.nx = G.nx;
+    L.ny = G.ny;
+    L.nz = G.nz;
+    L.per_x = bc.type[0] == MF3D_BC_PERIODIC;
+    L.per_y = bc.type[2] == MF3D_BC_PERIODIC;
+    L.per_z = bc.type[4] == MF3D_BC_PERIODIC;
+    L.pin = pin ? 1 : 0;
+    L.dx2 = G.dx * G.dx / scale;
+    L.inv_dx2 = scale / (G.dx * G.dx);
+    return L;
+}
+
+// Coefficient storage of one level in precision TC.
+struct CoefStore {
+    DevMem mem;
+    template <class TC> void build(const Geom& G, size_t elt, LevelOp<TC>& L) {
+        const size_t pl = (size_t)G.ny * G.nz + (size_t)G.nx * G.nz + (size_t)G.nx * G.ny;
+        mem.alloc((3 * G.n + pl) * elt + 256);
+        char* p = mem.as<char>();
+        L.cx = (const TC*)p;
+        L.cy = (const TC*)(p + G.n * elt);
+        L.cz = (const TC*)(p + 2 * G.n * elt);
+        L.bxm = (const TC*)(p + 3 * G.n * elt);
+        L.bym = L.bxm + (size_t)G.ny * G.nz;
+        L.bzm = L.bym + (size_t)G.nx * G.nz;
+    }
+};
+
+template <class TC>
+static void launch_faces(cudaStream_t s, const Geom& G, const double* K, const mf3d_bc& bc, double scale,
+                         const LevelOp<TC>& L) {
+    faces_kernel<TC><<<grid1d(G.n, 256), 256, 0, s>>>(G.nx, G.ny, G.nz, K, to_dev(bc), scale, (TC*)L.cx,
+                                                       (TC*)L.cy, (TC*)L.cz, (TC*)L.bxm, (TC*)L.bym, (TC*)L.bzm);
+    MF3D_LAUNCH_CK();
+}
+
+// Power-of-two scale for a bf16 level: 2^-round(log2 of the level's typical coefficient)
+// keeps the stored values centred on 1 (bf16 has float's exponent range, so the scale is a
+// tested variant, not a range fix).
+static double bf16_scale(const Geom& G) {
+    (void)G;
+    return 1.0;
+}
+
+// ---------------------------------------------------------------------------------------
+// V-cycle program for levels [0, Lt) in precision (T, TC) plus the FP64 tail [Lt, nl)
+// ---------------------------------------------------------------------------------------
+struct Timer {
+    cudaEvent_t e0, e1;
+    cudaStream_t s;
+    template <class F> float mean_ms(int reps, F&& f) {
+        f(); // warm-up launch
+        MF3D_CK(cudaEventRecord(e0, s));
+        for (int i = 0; i < reps; ++i) f();
+        MF3D_CK(cudaEventRecord(e1, s));
+        MF3D_CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        MF3D_CK(cudaEventElapsedTime(&ms, e0, e1));
+        return ms / reps;
+    }
+};
+
+static mf3d_kernel_timing timing(const char* name, float ms, double bytes, int per_iter) {
+    mf3d_kernel_timing t{};
+    std::snprintf(t.name, sizeof(t.name), "%s", name);
+    t.ms = ms;
+    t.bytes = bytes;
+    t.launches_per_iter = per_iter;
+    return t;
+}
+
+struct VCycleBase {
+    virtual ~VCycleBase() {}
+    virtual void build_coefs(cudaStream_t s, const std::vector<const double*>& Klev) = 0;
+    // z (type T) = V-cycle(r); if rho_out != null, <r, z> is summed into *rho_out.
+    virtual void run(cudaStream_t s, const double* r, void* z, double* rho_out) = 0;
+    // per-kernel timings of one V-cycle (level-0 sweeps by role, the coarse tail, the whole cycle)
+    virtual void profile(Timer& tm, int reps, const double* r, void* z, double* rho_out,
+                         std::vector<mf3d_kernel_timing>& out) = 0;
+    virtual size_t z_elt() const = 0;
+    virtual size_t bytes() const = 0;
+};
+
+struct Scratch {
+    double* partials;
+    unsigned* tickets; // one per reduction site
+    size_t partial_cap;
+};
+
+template <class T, class TC> class VCycle : public VCycleBase {
+  public:
+    VCycle(const std::vector<Geom>& G, int Lt, const mf3d_bc& bc, bool pin, int pre, int post, int coarse,
+           const std::vector<LevelOp<double>>& op64, Scratch scr)
+        : G_(G), Lt_(Lt), bc_(bc), pin_(pin), pre_(pre), post_(post), coarse_(coarse), op64_(op64), scr_(scr) {
+        const int nl = (int)G.size();
+        ops_.resize(Lt);
+        coef_.resize(Lt);
+        xa_.resize(Lt);
+        xb_.resize(Lt);
+        bl_.resize(Lt + 1);
+        for (int l = 0; l < Lt; ++l) {
+            scale_.push_back(std::is_same<TC, __nv_bfloat16>::value ? bf16_scale(G[l]) : 1.0);
+            ops_[l] = make_op<TC>(G[l], bc, pin, scale_[l]);
+            if (std::is_same<TC, double>::value) {
+                // FP64 V-cycle shares the FP64 coefficients
+                const LevelOp<double>& o = op64[l];
+                ops_[l].cx = (const TC*)o.cx;
+                ops_[l].cy = (const TC*)o.cy;
+                ops_[l].cz = (const TC*)o.cz;
+                ops_[l].bxm = (const TC*)o.bxm;
+                ops_[l].bym = (const TC*)o.bym;
+                ops_[l].bzm = (const TC*)o.bzm;
+            } else {
+                coef_[l].reset(new CoefStore());
+                coef_[l]->build<TC>(G[l], sizeof(TC), ops_[l]);
+                bytes_ += coef_[l]->mem.bytes;
+            }
+            xa_[l].reset(new DevMem(G[l].n * sizeof(T)));
+            xb_[l].reset(new DevMem(G[l].n * sizeof(T)));
+            bytes_ += 2 * G[l].n * sizeof(T);
+        }
+        for (int l = 1; l <= Lt && l < nl; ++l) {
+            bl_[l].reset(new DevMem(G[l].n * sizeof(T)));
+            bytes_ += G[l].n * sizeof(T);
+        }
+        // tail
+        if (Lt < nl) {
+            tail_.nlev = nl - Lt;
+            if (tail_.nlev > TAIL_MAX_LEVELS) throw Error(MF3D_E_INVALID, "too many coarse tail levels");
+            int off = 0;
+            for (int l = Lt; l < nl; ++l) {
+                tail_.L[l - Lt] = op64[l];
+                tail_.off[l - Lt] = off;
+                off += 2 * (int)G[l].n;
+            }
+            tail_.pre = pre;
+            tail_.post = post;
+            tail_.coarse_iters = coarse;
+            tail_smem_ = (size_t)off * sizeof(double);
+            tail_out_.reset(new DevMem(G[Lt].n * sizeof(T)));
+            bytes_ += G[Lt].n * sizeof(T);
+            if (tail_smem_ > 48 * 1024) {
+                MF3D_CK(cudaFuncSetAttribute(tail_kernel<T, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)tail_smem_));
+                MF3D_CK(cudaFuncSetAttribute(tail_kernel<double, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)tail_smem_));
+            }
+        }
+    }
+
+    void build_coefs(cudaStream_t s, const std::vector<const double*>& Klev) override {
+        if (std::is_same<TC, double>::value) return;
+        for (int l = 0; l < Lt_; ++l) launch_faces<TC>(s, G_[l], Klev[l], bc_, scale_[l], ops_[l]);
+    }
+
+    size_t z_elt() const override { return sizeof(T); }
+    size_t bytes() const override { return bytes_; }
+
+    void run(cudaStream_t s, const double* r, void* zv, double* rho_out) override {
+        T* z = (T*)zv;
+        const int nl = (int)G_.size();
+        std::vector<const T*> cur(Lt_ + 1, nullptr), fin(Lt_ + 1, nullptr);
+        // ---- down ----
+        for (int l = 0; l < Lt_; ++l) {
+            T* bc_next = (T*)bl_[l + 1]->p;
+            const T* c = nullptr;
+            for (int sw = 1; sw <= pre_; ++sw) {
+                T* out = (c == (const T*)xa_[l]->p) ? (T*)xb_[l]->p : (T*)xa_[l]->p;
+                int mode = (c ? 0 : M_ZERO) | (sw == pre_ ? M_RESID : 0);
+                sweep(s, l, r, c, out, nullptr, bc_next, mode, nullptr);
+                c = out;
+            }
+            if (pre_ == 0) restrict_b(s, l, r, bc_next);
+            cur[l] = c;
+        }
+        // ---- tail (coarsest levels in one CTA, FP64) ----
+        const T* e_below = nullptr;
+        if (Lt_ < nl) {
+            T* out = (Lt_ == 0) ? z : (T*)tail_out_->p;
+            if (Lt_ == 0) {
+                tail_kernel<double, T><<<1, TAIL_NT, tail_smem_, s>>>(tail_, r, out);
+            } else {
+                tail_kernel<T, T><<<1, TAIL_NT, tail_smem_, s>>>(tail_, (const T*)bl_[Lt_]->p, out);
+            }
+            MF3D_LAUNCH_CK();
+            e_below = out;
+            if (Lt_ == 0 && rho_out) dot_rz(s, r, z, G_[0].n, rho_out);
+        }
+        // ---- up ----
+        for (int l = Lt_ - 1; l >= 0; --l) {
+            const T* c = cur[l];
+            const T* e = (l + 1 == Lt_) ? e_below : fin[l + 1];
+            for (int sw = 1; sw <= post_; ++sw) {
+                const bool last = sw == post_;
+                T* out;
+                if (l == 0 && last) out = z;
+                else out = (c == (const T*)xa_[l]->p) ? (T*)xb_[l]->p : (T*)xa_[l]->p;
+                int mode = (c ? 0 : M_ZERO) | (sw == 1 ? M_PROLONG : 0) | ((l == 0 && last && rho_out) ? M_DOT : 0);
+                sweep(s, l, r, c, out, e, nullptr, mode, rho_out);
+                c = out;
+            }
+            if (post_ == 0) {
+                T* out = (l == 0) ? z : ((c == (const T*)xa_[l]->p) ? (T*)xb_[l]->p : (T*)xa_[l]->p);
+                prolong_kernel<T><<<grid1d(G_[l].n, 256), 256, 0, s>>>(G_[l].nx, G_[l].ny, G_[l].nz, c, e, out);
+                MF3D_LAUNCH_CK();
+                c = out;
+                if (l == 0 && rho_out) dot_rz(s, r, z, G_[0].n, rho_out);
+            }
+            fin[l] = c;
+        }
+    }
+
+    void profile(Timer& tm, int reps, const double* r, void* zv, double* rho_out,
+                 std::vector<mf3d_kernel_timing>& out) override {
+        T* z = (T*)zv;
+        const int nl = (int)G_.size();
+        out.push_back(timing("vcycle_total", tm.mean_ms(reps, [&] { run(tm.s, r, zv, rho_out); }), 0.0, 1));
+        if (Lt_ >= 1) {
+            const double n = (double)G_[0].n, et = sizeof(T), ec = sizeof(TC);
+            const double coef = 3.0 * n * ec, nc = n / 8.0;
+            T* xa = (T*)xa_[0]->p;
+            T* xb = (T*)xb_[0]->p;
+            T* bc1 = (T*)bl_[1]->p;
+            const T* e1 = (Lt_ == 1) ? (const T*)tail_out_->p : (const T*)xa_[1]->p;
+            const int pre_extra = std::max(0, pre_ - 2), post_extra = std::max(0, post_ - 2);
+            if (pre_ >= 1) {
+                out.push_back(timing("sweep_l0_zero_in", tm.mean_ms(reps, [&] {
+                    sweep(tm.s, 0, r, nullptr, xa, nullptr, bc1, pre_ == 1 ? (M_ZERO | M_RESID) : M_ZERO, nullptr);
+                }), 8.0 * n + coef + et * n + (pre_ == 1 ? et * nc : 0.0), 1));
+            }
+            if (pre_ >= 2) {
+                out.push_back(timing("sweep_l0_resid_restrict", tm.mean_ms(reps, [&] {
+                    sweep(tm.s, 0, r, xa, xb, nullptr, bc1, M_RESID, nullptr);
+                }), et * n + 8.0 * n + coef + et * n + et * nc, 1));
+            }
+            if (pre_extra + post_extra > 0) {
+                out.push_back(timing("sweep_l0_plain", tm.mean_ms(reps, [&] {
+                    sweep(tm.s, 0, r, xa, xb, nullptr, nullptr, 0, nullptr);
+                }), et * n + 8.0 * n + coef + et * n, pre_extra + post_extra));
+            }
+            if (post_ >= 2) {
+                out.push_back(timing("sweep_l0_prolong", tm.mean_ms(reps, [&] {
+                    sweep(tm.s, 0, r, xb, xa, e1, nullptr, M_PROLONG, nullptr);
+                }), et * n + et * nc + 8.0 * n + coef + et * n, 1));
+            }
+            if (post_ >= 1) {
+                out.push_back(timing("sweep_l0_dot_out", tm.mean_ms(reps, [&] {
+                    sweep(tm.s, 0, r, xa, z, e1, nullptr, post_ == 1 ? (M_PROLONG | M_DOT) : M_DOT, rho_out);
+                }), et * n + 8.0 * n + coef + et * n + (post_ == 1 ? et * nc : 0.0), 1));
+            }
+            // every other sweep level, whole
+            for (int l = 1; l < Lt_; ++l) {
+                char nm[40];
+                std::snprintf(nm, sizeof(nm), "sweep_l%d_plain", l);
+                T* a = (T*)xa_[l]->p;
+                T* b = (T*)xb_[l]->p;
+                const double nn = (double)G_[l].n;
+                out.push_back(timing(nm, tm.mean_ms(reps, [&] { sweep(tm.s, l, r, a, b, nullptr, nullptr, 0, nullptr); }),
+                                     3.0 * et * nn + 3.0 * nn * ec, pre_ + post_));
+            }
+        }
+        if (Lt_ < nl) {
+            T* outp = (Lt_ == 0) ? z : (T*)tail_out_->p;
+            out.push_back(timing("coarse_tail", tm.mean_ms(reps, [&] {
+                if (Lt_ == 0)
+                    tail_kernel<double, T><<<1, TAIL_NT, tail_smem_, tm.s>>>(tail_, r, outp);
+                else
+                    tail_kernel<T, T><<<1, TAIL_NT, tail_smem_, tm.s>>>(tail_, (const T*)bl_[Lt_]->p, outp);
+                MF3D_LAUNCH_CK();
+            }), 0.0, 1));
+        }
+    }
+
+  private:
+    static int zchunk_for(const Geom& g, int nblk_xy) {
+        const int target = num_sms() * 6;
+        int zc = (int)((long long)g.nz * nblk_xy / std::max(1, target));
+        zc = std::max(8, (zc + 1) & ~1);
+        return std::min(zc, ((g.nz + 1) & ~1));
+    }
+
+    void sweep(cudaStream_t s, int l, const double* r, const T* x_in, T* x_out, const T* e, T* b_coarse, int mode,
+               double* dot_out) {
+        const Geom& g = G_[l];
+        const int gx = (g.nx + SW_TX - 1) / SW_TX, gy = (g.ny + SW_TY - 1) / SW_TY;
+        const int zc = zchunk_for(g, gx * gy);
+        const int gz = (g.nz + zc - 1) / zc;
+        dim3 grid(gx, gy, gz);
+        const unsigned nblk = (unsigned)gx * gy * gz;
+        if ((mode & M_DOT) && nblk > scr_.partial_cap) throw Error(MF3D_E_INVALID, "reduction scratch too small");
+        if (l == 0) {
+            SweepArgs<T, TC, double> a{};
+            fill(a, l, r, x_in, x_out, e, b_coarse, zc, dot_out);
+            dispatch<double>(s, grid, mode, a);
+        } else {
+            SweepArgs<T, TC, T> a{};
+            fill(a, l, (const T*)bl_[l]->p, x_in, x_out, e, b_coarse, zc, dot_out);
+            dispatch<T>(s, grid, mode, a);
+        }
+    }
+
+    template <class TB>
+    void fill(SweepArgs<T, TC, TB>& a, int l, const TB* b, const T* x_in, T* x_out, const T* e, T* b_coarse, int zc,
+              double* dot_out) {
+        a.L = ops_[l];
+        a.b = b;
+        a.x_in = x_in;
+        a.x_out = x_out;
+        a.e_c = e;
+        if (l + 1 < (int)G_.size()) {
+            a.ncx = G_[l + 1].nx;
+            a.ncy = G_[l + 1].ny;
+        }
+        a.b_coarse = b_coarse;
+        a.zchunk = zc;
+        a.dot_partials = scr_.partials;
+        a.dot_ticket = scr_.tickets + 0;
+        a.dot_out = dot_out;
+    }
+
+    template <class TB> void dispatch(cudaStream_t s, dim3 grid, int mode, const SweepArgs<T, TC, TB>& a) {
+        switch (mode) {
+        case 0: sweep_kernel<T, TC, TB, 0><<<grid, SW_NT, 0, s>>>(a); break;
+        case M_ZERO: sweep_kernel<T, TC, TB, M_ZERO><<<grid, SW_NT, 0, s>>>(a); break;
+        case M_PROLONG: sweep_kernel<T, TC, TB, M_PROLONG><<<grid, SW_NT, 0, s>>>(a); break;
+        case M_ZERO | M_PROLONG: sweep_kernel<T, TC, TB, M_ZERO | M_PROLONG><<<grid, SW_NT, 0, s>>>(a); break;
+        case M_RESID: sweep_kernel<T, TC, TB, M_RESID><<<grid, SW_NT, 0, s>>>(a); break;
+        case M_ZERO | M_RESID: sweep_kernel<T, TC, TB, M_ZERO | M_RESID><<<grid, SW_NT, 0, s>>>(a); break;
+        case M_DOT: sweep_kernel<T, TC, TB, M_DOT><<<grid, SW_NT, 0, s>>>(a); break;
+        case M_ZERO | M_DOT: sweep_kernel<T, TC, TB, M_ZERO | M_DOT><<<grid, SW_NT, 0, s>>>(a); break;
+        case M_PROLONG | M_DOT: sweep_kernel<T, TC, TB, M_PROLONG | M_DOT><<<grid, SW_NT, 0, s>>>(a); break;
+        case M_ZERO | M_PROLONG | M_DOT:
+            sweep_kernel<T, TC, TB, M_ZERO | M_PROLONG | M_DOT><<<grid, SW_NT, 0, s>>>(a);
+            break;
+        default: throw Error(MF3D_E_INVALID, "unsupported sweep mode");
+        }
+        MF3D_LAUNCH_CK();
+    }
+
+    void restrict_b(cudaStream_t s, int l, const double* r, T* out) {
+        const Geom& c = G_[l + 1];
+        if (l == 0)
+            restrict_kernel<T, double><<<grid1d(c.n, 256), 256, 0, s>>>(c.nx, c.ny, c.nz, r, out);
+        else
+            restrict_kernel<T, T><<<grid1d(c.n, 256), 256, 0, s>>>(c.nx, c.ny, c.nz, (const T*)bl_[l]->p, out);
+        MF3D_LAUNCH_CK();
+    }
+
+    void dot_rz(cudaStream_t s, const double* r, const T* z, size_t n, double* out);
+
+    std::vector<Geom> G_;
+    int Lt_;
+    mf3d_bc bc_;
+    bool pin_;
+    int pre_, post_, coarse_;
+    std::vector<LevelOp<double>> op64_;
+    Scratch scr_;
+    std::vector<LevelOp<TC>> ops_;
+    std::vector<double> scale_;
+    std::vector<std::unique_ptr<CoefStore>> coef_;
+    std::vector<std::unique_ptr<DevMem>> xa_, xb_, bl_;
+    std::unique_ptr<DevMem> tail_out_;
+    TailArgs tail_{};
+    size_t tail_smem_ = 0;
+    size_t bytes_ = 0;
+};
+
+template <class T>
+__global__ void dot_kernel(size_t n, const double* __restrict__ a, const T* __restrict__ b, double* partials,
+                           unsigned* ticket, double* out) {
+    double acc = 0.0;
+    for (size_t c = blockIdx.x * (size_t)PK_NT + threadIdx.x; c < n; c += (size_t)gridDim.x * PK_NT)
+        acc += a[c] * (double)b[c];
+    double v[1] = {acc}, o[1];
+    if (grid_sums<PK_NT, 1>(v, partials, ticket, gridDim.x, o)) *out = o[0];
+}
+
+template <class T, class TC>
+void VCycle<T, TC>::dot_rz(cudaStream_t s, const double* r, const T* z, size_t n, double* out) {
+    const unsigned nb = std::min<unsigned>(grid1d(n, PK_NT), (unsigned)scr_.partial_cap);
+    dot_kernel<T><<<nb, PK_NT, 0, s>>>(n, r, z, scr_.partials, scr_.tickets + 1, out);
+    MF3D_LAUNCH_CK();
+}
+
+// ---------------------------------------------------------------------------------------
+// HeadSolver
+// ---------------------------------------------------------------------------------------
+class HeadSolver {
+  public:
+    HeadSolver(const mf3d_grid& g, const mf3d_bc& bc, const mf3d_solver_config& cfg, cudaStream_t user_stream)
+        : grid_(g), bc_(bc), cfg_(cfg) {
+        if (g.nx < 2 || g.ny < 2 || g.nz < 2) throw Error(MF3D_E_INVALID, "grid must have at least 2 cells per axis");
+        if (!(g.dx > 0)) throw Error(MF3D_E_INVALID, "dx must be positive");
+        validate_bc(bc);
+        if (cfg.solver != MF3D_SOLVER_PCG_MG)
+            throw Error(MF3D_E_INVALID, "only the PCG_MG solver is implemented on this path");
+        if (cfg.mg_pre_smooth < 0 || cfg.mg_post_smooth < 0 || cfg.mg_coarse_iters < 0 || cfg.cg_max_iter < 0)
+            throw Error(MF3D_E_INVALID, "negative iteration count");
+        for (int a = 0; a < 3; ++a) {
+            const int n = a == 0 ? g.nx : (a == 1 ? g.ny : g.nz);
+            if (bc.type[2 * a] == MF3D_BC_PERIODIC && (n & 1))
+                throw Error(MF3D_E_INVALID, "red-black smoothing needs an even cell count on a periodic axis");
+        }
+        pin_ = pin_enabled(cfg.pin_mode, bc);
+        G_ = make_levels(g, cfg.mg_levels);
+        const int nl = (int)G_.size();
+        // coarse tail: the smallest suffix of levels whose x and b fit in shared memory
+        Lt_ = nl - 1;
+        size_t cells = G_[nl - 1].n;
+        while (Lt_ > 0 && G_[Lt_ - 1].n <= 4096 && cells + G_[Lt_ - 1].n <= 12288) {
+            --Lt_;
+            cells += G_[Lt_].n;
+        }
+        if (cells > 12288) throw Error(MF3D_E_INVALID, "coarsest level too large for the coarse solver "
+                                                       "(raise mg_levels)");
+        if (user_stream) {
+            stream_ = user_stream;
+        } else {
+            MF3D_CK(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
+            stream_ = own_stream_;
+        }
+        const size_t n = G_[0].n;
+        // FP64 operator coefficients: level 0 (PCG operator), tail levels, and every level of an
+        // FP64 V-cycle.
+        op64_.resize(nl);
+        coef64_.resize(nl);
+        for (int l = 0; l < nl; ++l) {
+            op64_[l] = make_op<double>(G_[l], bc, pin_, 1.0);
+            if (l == 0 || l >= Lt_ || cfg.precision == MF3D_PREC_FP64) {
+                coef64_[l].reset(new CoefStore());
+                coef64_[l]->build<double>(G_[l], sizeof(double), op64_[l]);
+                bytes_ += coef64_[l]->mem.bytes;
+            }
+        }
+        Klev_.resize(nl);
+        for (int l = 0; l < nl; ++l) {
+            Klev_[l].reset(new DevMem(G_[l].n * sizeof(double)));
+            bytes_ += G_[l].n * sizeof(double);
+        }
+        auto vec = [&](DevMem& m) {
+            m.alloc(n * sizeof(double));
+            bytes_ += m.bytes;
+        };
+        vec(x_);
+        vec(b_);
+        vec(r_);
+        vec(p_);
+        vec(Ap_);
+        vec(x0_);
+        // reduction scratch sized for the largest grid any reduction uses
+        size_t cap = (size_t)grid1d(n, PK_NT) * 2 + 1024;
+        {
+            const int gx = (G_[0].nx + SW_TX - 1) / SW_TX, gy = (G_[0].ny + SW_TY - 1) / SW_TY;
+            cap = std::max(cap, (size_t)gx * gy * (size_t)((G_[0].nz + 7) / 8) + 1024);
+        }
+        partials_.alloc(cap * 2 * sizeof(double));
+        tickets_.alloc(16 * sizeof(unsigned));
+        state_.alloc(sizeof(PcgState));
+        mb_.alloc(4 * sizeof(double));
+        MF3D_CK(cudaMemsetAsync(tickets_.p, 0, tickets_.bytes, stream_));
+        MF3D_CK(cudaMemsetAsync(state_.p, 0, state_.bytes, stream_));
+        bytes_ += partials_.bytes;
+        Scratch scr{partials_.as<double>(), tickets_.as<unsigned>() + 8, cap};
+        const int prec = cfg.precision;
+        if (prec == MF3D_PREC_FP64)
+            vc_.reset(new VCycle<double, double>(G_, Lt_, bc, pin_, cfg.mg_pre_smooth, cfg.mg_post_smooth,
+                                                 cfg.mg_coarse_iters, op64_, scr));
+        else if (prec == MF3D_PREC_FP32)
+            vc_.reset(new VCycle<float, float>(G_, Lt_, bc, pin_, cfg.mg_pre_smooth, cfg.mg_post_smooth,
+                                               cfg.mg_coarse_iters, op64_, scr));
+        else if (prec == MF3D_PREC_BF16)
+            vc_.reset(new VCycle<float, __nv_bfloat16>(G_, Lt_, bc, pin_, cfg.mg_pre_smooth, cfg.mg_post_smooth,
+                                                       cfg.mg_coarse_iters, op64_, scr));
+        else
+            throw Error(MF3D_E_INVALID, "unknown precision");
+        bytes_ += vc_->bytes();
+        z_.alloc(n * vc_->z_elt());
+        bytes_ += z_.bytes;
+        flexible_ = cfg.flexible < 0 ? (prec != MF3D_PREC_FP64) : (cfg.flexible != 0);
+        host_state_ = nullptr;
+        MF3D_CK(cudaMallocHost(&host_state_, sizeof(PcgState)));
+        MF3D_CK(cudaEventCreate(&ev0_));
+        MF3D_CK(cudaEventCreate(&ev1_));
+        MF3D_CK(cudaStreamSynchronize(stream_));
+    }
+
+    ~HeadSolver() {
+        if (loop_exec_) cudaGraphExecDestroy(loop_exec_);
+        if (loop_graph_) cudaGraphDestroy(loop_graph_);
+        if (host_state_) cudaFreeHost(host_state_);
+        if (ev0_) cudaEventDestroy(ev0_);
+        if (ev1_) cudaEventDestroy(ev1_);
+        if (own_stream_) {
+            cudaStreamSynchronize(own_stream_);
+            cudaStreamDestroy(own_stream_);
+        }
+    }
+
+    int num_levels() const { return (int)G_.size(); }
+    long long device_bytes() const { return (long long)bytes_; }
+
+    void set_K(const double* K) {
+        if (!K) throw Error(MF3D_E_INVALID, "K is null");
+        const long long l0 = g_launches;
+        cudaStream_t s = stream_;
+        const int nl = (int)G_.size();
+        MF3D_CK(cudaMemcpyAsync(Klev_[0]->p, K, G_[0].n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        for (int l = 0; l + 1 < nl; ++l) {
+            const Geom& c = G_[l + 1];
+            coarsen_kernel<<<grid1d(c.n, 256), 256, 0, s>>>(c.nx, c.ny, c.nz, Klev_[l]->as<double>(),
+                                                            Klev_[l + 1]->as<double>());
+            MF3D_LAUNCH_CK();
+        }
+        std::vector<const double*> Kp(nl);
+        for (int l = 0; l < nl; ++l) Kp[l] = Klev_[l]->as<double>();
+        for (int l = 0; l < nl; ++l)
+            if (coef64_[l]) launch_faces<double>(s, G_[l], Kp[l], bc_, 1.0, op64_[l]);
+        vc_->build_coefs(s, Kp);
+        rhs_guess_kernel<<<grid1d(G_[0].n, 256), 256, 0, s>>>(G_[0].nx, G_[0].ny, G_[0].nz, G_[0].dx, Kp[0],
+                                                              to_dev(bc_), b_.as<double>(), x0_.as<double>());
+        MF3D_LAUNCH_CK();
+        setup_launches_ = (int)(g_launches - l0);
+        have_K_ = true;
+    }
+
+    int setup_launches() const { return setup_launches_; }
+
+    void vcycle(const double* r, double* z) {
+        if (!have_K_) throw Error(MF3D_E_STATE, "set_K must be called before vcycle");
+        if (vc_->z_elt() == sizeof(double)) {
+            vc_->run(stream_, r, z, nullptr);
+        } else {
+            vc_->run(stream_, r, z_.p, nullptr);
+            convert_kernel<double, float><<<grid1d(G_[0].n, 256), 256, 0, stream_>>>(G_[0].n, z_.as<float>(), z);
+            MF3D_LAUNCH_CK();
+        }
+        MF3D_CK(cudaStreamSynchronize(stream_));
+    }
+
+    void solve(double* h, const double* x0, mf3d_solve_result* res) {
+        if (!have_K_) throw Error(MF3D_E_STATE, "set_K must be called before solve");
+        if (!h) throw Error(MF3D_E_INVALID, "h is null");
+        cudaStream_t s = stream_;
+        const size_t n = G_[0].n;
+        const long long l0 = g_launches;
+        long long body_runs = 0;
+        MF3D_CK(cudaEventRecord(ev0_, s));
+        MF3D_CK(cudaMemcpyAsync(x_.p, x0 ? x0 : x0_.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        MF3D_CK(cudaMemsetAsync(tickets_.p, 0, tickets_.bytes, s));
+        pcg_init_kernel<<<1, 1, 0, s>>>(state_.as<PcgState>(), cfg_.cg_max_iter, cfg_.cg_check_every,
+                                        flexible_ ? 1 : 0, cfg_.cg_rtol, kSolveBudgetNs);
+        MF3D_LAUNCH_CK();
+        launch_residual(s, 0);
+        if (cfg_.use_graph) {
+            if (!loop_exec_) build_loop_graph();
+            MF3D_CK(cudaGraphLaunch(loop_exec_, s));
+            body_runs = -1; // known once the iteration count is back
+        } else {
+            // host-driven loop: one iteration per launch sequence, stop flag polled each time
+            for (int it = 0; it < std::max(cfg_.cg_max_iter, 1); ++it) {
+                record_body(s, false);
+                ++body_runs;
+                MF3D_CK(cudaMemcpyAsync(host_state_, state_.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
+                MF3D_CK(cudaStreamSynchronize(s));
+                if (host_state_->stop) break;
+            }
+        }
+        launch_residual(s, 1);
+        MF3D_CK(cudaMemcpyAsync(h, x_.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        MF3D_CK(cudaEventRecord(ev1_, s));
+        MF3D_CK(cudaMemcpyAsync(host_state_, state_.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
+        MF3D_CK(cudaStreamSynchronize(s));
+        const PcgState& st = *host_state_;
+        long long launches = g_launches - l0;
+        if (body_runs < 0) launches += (long long)std::max(st.iter, 1) * body_launches_;
+        if (res) {
+            std::memset(res, 0, sizeof(*res));
+            res->num_iterations = st.iter;
+            res->converged = st.converged;
+            res->status = st.status;
+            res->num_levels = (int)G_.size();
+            res->initial_residual = std::sqrt(st.r0sq);
+            res->final_residual = st.final_res;
+            res->b_norm = std::sqrt(st.bb);
+            res->true_rel_residual = st.bb > 0 ? std::sqrt(st.rr_true / st.bb) : std::sqrt(st.rr_true);
+            float ms = 0.f;
+            MF3D_CK(cudaEventElapsedTime(&ms, ev0_, ev1_));
+            res->device_ms = ms;
+            res->kernel_launches = (int)launches;
+        }
+    }
+
+    // Times each kernel of one PCG iteration on the current state (see mf3d.h).
+    std::vector<mf3d_kernel_timing> profile(int reps) {
+        if (!have_K_) throw Error(MF3D_E_STATE, "set_K must be called before profile");
+        Timer tm{ev0_, ev1_, stream_};
+        std::vector<mf3d_kernel_timing> out;
+        const size_t n = G_[0].n;
+        PcgState* st = state_.as<PcgState>();
+        const double nd = (double)n, ez = (double)vc_->z_elt();
+        vc_->profile(tm, reps, r_.as<double>(), z_.p, &st->rho_new, out);
+        const unsigned nb = grid1d(n, PK_NT);
+        out.push_back(timing("matvec_dot", tm.mean_ms(reps, [&] {
+            matvec_dot_kernel<double><<<nb, PK_NT, 0, stream_>>>(op64_[0], p_.as<double>(), Ap_.as<double>(), st,
+                                                                 partials_.as<double>(), tickets_.as<unsigned>() + 3);
+            MF3D_LAUNCH_CK();
+        }), 40.0 * nd, 1));
+        out.push_back(timing("residual_true", tm.mean_ms(reps, [&] { launch_residual(stream_, 1); }), 48.0 * nd, 0));
+        out.push_back(timing("pupdate", tm.mean_ms(reps, [&] {
+            if (vc_->z_elt() == sizeof(double))
+                pupdate_kernel<double><<<nb, PK_NT, 0, stream_>>>(n, z_.as<double>(), p_.as<double>(), st);
+            else
+                pupdate_kernel<float><<<nb, PK_NT, 0, stream_>>>(n, z_.as<float>(), p_.as<double>(), st);
+            MF3D_LAUNCH_CK();
+        }), ez * nd + 16.0 * nd, 1));
+        out.push_back(timing("xr_update", tm.mean_ms(reps, [&] {
+            if (vc_->z_elt() == sizeof(double))
+                xr_update_kernel<double><<<nb, PK_NT, 0, stream_>>>(n, x_.as<double>(), p_.as<double>(), r_.as<double>(),
+                                                                   Ap_.as<double>(), z_.as<double>(), st,
+                                                                   partials_.as<double>(), tickets_.as<unsigned>() + 4,
+                                                                   cond_, 0);
+            else
+                xr_update_kernel<float><<<nb, PK_NT, 0, stream_>>>(n, x_.as<double>(), p_.as<double>(), r_.as<double>(),
+                                                                  Ap_.as<double>(), z_.as<float>(), st,
+                                                                  partials_.as<double>(), tickets_.as<unsigned>() + 4,
+                                                                  cond_, 0);
+            MF3D_LAUNCH_CK();
+        }), 48.0 * nd + (flexible_ ? ez * nd : 0.0), 1));
+        return out;
+    }
+
+    cudaStream_t stream() const { return stream_; }
+
+  private:
+    void launch_residual(cudaStream_t s, int mode) {
+        const size_t n = G_[0].n;
+        double* out = mode == 0 ? r_.as<double>() : Ap_.as<double>();
+        residual_kernel<double><<<grid1d(n, PK_NT), PK_NT, 0, s>>>(
+            op64_[0], x_.as<double>(), b_.as<double>(), out, state_.as<PcgState>(), partials_.as<double>(),
+            tickets_.as<unsigned>() + 2, mode, cfg_.conv_norm == MF3D_CONV_B ? 1 : 0);
+        MF3D_LAUNCH_CK();
+    }
+
+    // One PCG iteration (loop body).
+    void record_body(cudaStream_t s, bool with_cond) {
+        const size_t n = G_[0].n;
+        PcgState* st = state_.as<PcgState>();
+        vc_->run(s, r_.as<double>(), z_.p, &st->rho_new);
+        const unsigned nb = grid1d(n, PK_NT);
+        if (vc_->z_elt() == sizeof(double)) {
+            pupdate_kernel<double><<<nb, PK_NT, 0, s>>>(n, z_.as<double>(), p_.as<double>(), st);
+        } else {
+            pupdate_kernel<float><<<nb, PK_NT, 0, s>>>(n, z_.as<float>(), p_.as<double>(), st);
+        }
+        MF3D_LAUNCH_CK();
+        matvec_dot_kernel<double><<<nb, PK_NT, 0, s>>>(op64_[0], p_.as<double>(), Ap_.as<double>(), st,
+                                                       partials_.as<double>(), tickets_.as<unsigned>() + 3);
+        MF3D_LAUNCH_CK();
+        if (vc_->z_elt() == sizeof(double)) {
+            xr_update_kernel<double><<<nb, PK_NT, 0, s>>>(n, x_.as<double>(), p_.as<double>(), r_.as<double>(),
+                                                          Ap_.as<double>(), z_.as<double>(), st,
+                                                          partials_.as<double>(), tickets_.as<unsigned>() + 4,
+                                                          cond_, with_cond ? 1 : 0);
+        } else {
+            xr_update_kernel<float><<<nb, PK_NT, 0, s>>>(n, x_.as<double>(), p_.as<double>(), r_.as<double>(),
+                                                         Ap_.as<double>(), z_.as<float>(), st,
+                                                         partials_.as<double>(), tickets_.as<unsigned>() + 4,
+                                                         cond_, with_cond ? 1 : 0);
+        }
+        MF3D_LAUNCH_CK();
+    }
+
+    void build_loop_graph() {
+        MF3D_CK(cudaGraphCreate(&loop_graph_, 0));
+        MF3D_CK(cudaGraphConditionalHandleCreate(&cond_, loop_graph_, 1u, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond_;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        MF3D_CK(cudaGraphAddNode(&node, loop_graph_, nullptr, 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        cudaStream_t cs;
+        MF3D_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        MF3D_CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        const long long l0 = g_launches;
+        try {
+            record_body(cs, true);
+            body_launches_ = (int)(g_launches - l0);
+            g_launches = l0; // captured, not launched
+        } catch (...) {
+            cudaGraph_t tmp;
+            cudaStreamEndCapture(cs, &tmp);
+            cudaStreamDestroy(cs);
+            throw;
+        }
+        cudaGraph_t tmp;
+        MF3D_CK(cudaStreamEndCapture(cs, &tmp));
+        MF3D_CK(cudaStreamDestroy(cs));
+        MF3D_CK(cudaGraphInstantiate(&loop_exec_, loop_graph_, 0));
+    }
+
+    mf3d_grid grid_;
+    mf3d_bc bc_;
+    mf3d_solver_config cfg_;
+    bool pin_ = false;
+    bool flexible_ = false;
+    bool have_K_ = false;
+    std::vector<Geom> G_;
+    int Lt_ = 0;
+    cudaStream_t stream_ = nullptr, own_stream_ = nullptr;
+    std::vector<LevelOp<double>> op64_;
+    std::vector<std::unique_ptr<CoefStore>> coef64_;
+    std::vector<std::unique_ptr<DevMem>> Klev_;
+    DevMem x_, b_, r_, p_, Ap_, x0_, z_;
+    DevMem partials_, tickets_, state_, mb_;
+    std::unique_ptr<VCycleBase> vc_;
+    PcgState* host_state_ = nullptr;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    cudaGraph_t loop_graph_ = nullptr;
+    cudaGraphExec_t loop_exec_ = nullptr;
+    cudaGraphConditionalHandle cond_ = 0;
+    size_t bytes_ = 0;
+    int setup_launches_ = 0, body_launches_ = 0;
+};
+
+// ---------------------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3",
+// SC'11), used for the K-field modes: counter = (mode, draw, 0, 0), key = seed.
+// ---------------------------------------------------------------------------------------
+struct Philox {
+    static void round(uint32_t c[4], uint32_t k[2]) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        const uint32_t n0 = hi1 ^ c[1] ^ k[0], n1 = lo1, n2 = hi0 ^ c[3] ^ k[1], n3 = lo0;
+        c[0] = n0;
+        c[1] = n1;
+        c[2] = n2;
+        c[3] = n3;
+        k[0] += 0x9E3779B9u;
+        k[1] += 0xBB67AE85u;
+    }
+    static void gen(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t out[4]) {
+        uint32_t c[4] = {c0, c1, 0u, 0u};
+        uint32_t k[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+        for (int r = 0; r < 10; ++r) round(c, k);
+        for (int q = 0; q < 4; ++q) out[q] = c[q];
+    }
+};
+
+// uniform double in (0,1) from 64 random bits
+static double u01(uint32_t a, uint32_t b) {
+    const uint64_t v = ((uint64_t)(a >> 5) << 26) | (uint64_t)(b >> 6); // 53 bits
+    return ((double)v + 0.5) / 9007199254740992.0;
+}
+
+struct ModeRng {
+    uint64_t seed;
+    uint32_t mode, draw = 0;
+    uint32_t buf[4];
+    int have = 0;
+    double next() {
+        if (have == 0) {
+            Philox::gen(seed, mode, draw++, buf);
+            have = 2;
+        }
+        const double u = have == 2 ? u01(buf[0], buf[1]) : u01(buf[2], buf[3]);
+        --have;
+        return u;
+    }
+};
+
+} // namespace mf3d
+
+// =========================================================================================
+// C-ABI
+// =========================================================================================
+using namespace mf3d;
+
+struct mf3d_head_solver {
+    std::unique_ptr<HeadSolver> impl;
+};
+
+template <class F> static int guard(F&& f) {
+    try {
+        f();
+        return MF3D_OK;
+    } catch (const Error& e) {
+        g_err = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_err = "host allocation failed";
+        return MF3D_E_NOMEM;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return MF3D_E_INVALID;
+    }
+}
+
+static void need(const void* p, const char* what) {
+    if (!p) throw Error(MF3D_E_INVALID, std::string(what) + " is null");
+}
+
+static void check_grid(const mf3d_grid* g) {
+    need(g, "grid");
+    if (g->nx < 1 || g->ny < 1 || g->nz < 1) throw Error(MF3D_E_INVALID, "grid sizes must be positive");
+    if (!(g->dx > 0)) throw Error(MF3D_E_INVALID, "dx must be positive");
+    if ((double)g->nx * g->ny * g->nz > 2147483647.0)
+        throw Error(MF3D_E_INVALID, "grid exceeds 2^31 cells");
+}
+
+extern "C" {
+
+const char* mf3d_last_error(void) { return g_err.c_str(); }
+const char* mf3d_version(void) { return "mf3d-b200 0.1 (sm_100a)"; }
+
+int mf3d_default_config(mf3d_solver_config* c) {
+    return guard([&] {
+        need(c, "cfg");
+        std::memset(c, 0, sizeof(*c));
+        c->solver = MF3D_SOLVER_PCG_MG;
+        c->mg_levels = 4;
+        c->mg_pre_smooth = 2;
+        c->mg_post_smooth = 2;
+        c->mg_max_cycles = 20;
+        c->mg_coarse_iters = 50;
+        c->cg_max_iter = 1000;
+        c->cg_check_every = 10;
+        c->cg_rtol = 1e-8;
+        c->rtol = 1e-6;
+        c->pin_mode = MF3D_PIN_AUTO;
+        c->precision = MF3D_PREC_FP64;
+        c->flexible = -1;
+        c->conv_norm = MF3D_CONV_R0;
+        c->use_graph = 1;
+    });
+}
+
+int mf3d_head_solver_create(const mf3d_grid* grid, const mf3d_bc* bc, const mf3d_solver_config* cfg, void* stream,
+                            mf3d_head_solver** out) {
+    return guard([&] {
+        check_grid(grid);
+        need(bc, "bc");
+        need(cfg, "cfg");
+        need(out, "out");
+        *out = nullptr;
+        std::unique_ptr<mf3d_head_solver> s(new mf3d_head_solver());
+        s->impl.reset(new HeadSolver(*grid, *bc, *cfg, (cudaStream_t)stream));
+        *out = s.release();
+    });
+}
+
+int mf3d_head_solver_destroy(mf3d_head_solver* s) {
+    return guard([&] { delete s; });
+}
+
+int mf3d_head_solver_num_levels(const mf3d_head_solver* s) { return s ? s->impl->num_levels() : MF3D_E_INVALID; }
+
+long long mf3d_head_solver_device_bytes(const mf3d_head_solver* s) { return s ? s->impl->device_bytes() : -1; }
+
+int mf3d_head_solver_set_K(mf3d_head_solver* s, const double* K) {
+    return guard([&] {
+        need(s, "solver");
+        s->impl->set_K(K);
+    });
+}
+
+int mf3d_head_solve(mf3d_head_solver* s, double* h, const double* x0, mf3d_solve_result* res) {
+    return guard([&] {
+        need(s, "solver");
+        s->impl->solve(h, x0, res);
+    });
+}
+
+int mf3d_head_solver_setup_launches(const mf3d_head_solver* s) {
+    return s ? s->impl->setup_launches() : MF3D_E_INVALID;
+}
+
+int mf3d_head_solver_profile(mf3d_head_solver* s, int reps, mf3d_kernel_timing* out, int cap, int* count) {
+    return guard([&] {
+        need(s, "solver");
+        need(out, "out");
+        need(count, "count");
+        auto v = s->impl->profile(std::max(1, reps));
+        *count = (int)std::min<size_t>(v.size(), (size_t)std::max(cap, 0));
+        for (int i = 0; i < *count; ++i) out[i] = v[i];
+    });
+}
+
+int mf3d_head_solver_vcycle(mf3d_head_solver* s, const double* r, double* z) {
+    return guard([&] {
+        need(s, "solver");
+        need(r, "r");
+        need(z, "z");
+        s->impl->vcycle(r, z);
+    });
+}
+
+static void run_velocity(const mf3d_grid* g, const mf3d_bc* bc, const double* h, const double* K, int layout,
+                         double* U, double* V, double* W, double* out_host, cudaStream_t s) {
+    check_grid(g);
+    need(bc, "bc");
+    validate_bc(*bc);
+    need(h, "h");
+    need(K, "K");
+    need(U, "U");
+    need(V, "V");
+    need(W, "W");
+    if (layout != MF3D_VEL_COMPACT && layout != MF3D_VEL_PADDED) throw Error(MF3D_E_INVALID, "unknown layout");
+    const size_t n = (size_t)g->nx * g->ny * g->nz;
+    VelOut o{U, V, W, layout};
+    if (!out_host) {
+        velocity_kernel<<<grid1d(n, VEL_NT), VEL_NT, 0, s>>>(g->nx, g->ny, g->nz, g->dx, h, K, to_dev(*bc), o,
+                                                             nullptr, nullptr, nullptr, nullptr);
+        MF3D_LAUNCH_CK();
+        return;
+    }
+    const unsigned nb = grid1d(n, VEL_NT);
+    DevMem scratch((size_t)nb * 2 * sizeof(double) + 64);
+    char* base = scratch.as<char>();
+    unsigned long long* mx = (unsigned long long*)base;
+    unsigned* ticket = (unsigned*)(base + 8);
+    double* sums = (double*)(base + 16);
+    double* partials = (double*)(base + 64);
+    MF3D_CK(cudaMemsetAsync(base, 0, 64, s));
+    velocity_kernel<<<nb, VEL_NT, 0, s>>>(g->nx, g->ny, g->nz, g->dx, h, K, to_dev(*bc), o, mx, partials, ticket, sums);
+    MF3D_LAUNCH_CK();
+    unsigned long long hb[4];
+    MF3D_CK(cudaMemcpyAsync(hb, base, 32, cudaMemcpyDeviceToHost, s));
+    MF3D_CK(cudaStreamSynchronize(s));
+    double d[3];
+    std::memcpy(&d[0], &hb[0], 8);
+    std::memcpy(&d[1], &hb[2], 8);
+    std::memcpy(&d[2], &hb[3], 8);
+    out_host[0] = d[0];
+    out_host[1] = d[1];
+    out_host[2] = d[2];
+}
+
+int mf3d_velocity_from_head(const mf3d_grid* g, const mf3d_bc* bc, const double* h, const double* K, int layout,
+                            double* U, double* V, double* W, void* stream) {
+    return guard([&] { run_velocity(g, bc, h, K, layout, U, V, W, nullptr, (cudaStream_t)stream); });
+}
+
+int mf3d_velocity_mass_balance(const mf3d_grid* g, const mf3d_bc* bc, const double* h, const double* K, double* U,
+                               double* V, double* W, double* out_host, void* stream) {
+    return guard([&] {
+        need(out_host, "out_host");
+        run_velocity(g, bc, h, K, MF3D_VEL_COMPACT, U, V, W, out_host, (cudaStream_t)stream);
+    });
+}
+
+// ---- operator pieces ----------------------------------------------------------------------
+struct OneLevel {
+    Geom G;
+    CoefStore cs;
+    LevelOp<double> op;
+    OneLevel(const mf3d_grid* g, const mf3d_bc* bc, int pin, const double* K, cudaStream_t s) {
+        check_grid(g);
+        need(bc, "bc");
+        validate_bc(*bc);
+        need(K, "K");
+        G = Geom{g->nx, g->ny, g->nz, (size_t)g->nx * g->ny * g->nz, g->dx};
+        op = make_op<double>(G, *bc, pin != 0, 1.0);
+        cs.build<double>(G, sizeof(double), op);
+        launch_faces<double>(s, G, K, *bc, 1.0, op);
+    }
+};
+
+__global__ void apply_A_kernel(const LevelOp<double> L, const double* __restrict__ x, double* __restrict__ y) {
+    const size_t n = (size_t)L.nx * L.ny * L.nz;
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c % L.nx), j = (int)((c / L.nx) % L.ny), k = (int)(c / ((size_t)L.nx * L.ny));
+        y[c] = apply_A_cell(L, x, i, j, k, c);
+    }
+}
+
+// r = b - A x with the smoother's pin convention (full diagonal doubled at cell 0,
+// src/multigrid/smoothers/residual_3d.cu:365-368).
+__global__ void residual_mg_kernel(const LevelOp<double> L, const double* __restrict__ x, const double* __restrict__ b,
+                                   double* __restrict__ r) {
+    const size_t n = (size_t)L.nx * L.ny * L.nz;
+    LevelOp<double> Lnp = L;
+    Lnp.pin = 0;
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c % L.nx), j = (int)((c / L.nx) % L.ny), k = (int)(c / ((size_t)L.nx * L.ny));
+        double ax = apply_A_cell(Lnp, x, i, j, k, c);
+        if (L.pin && c == 0) {
+            double cxm, cxp, cym, cyp, czm, czp;
+            cell_coefs<double>(L, i, j, k, c, cxm, cxp, cym, cyp, czm, czp);
+            ax -= (cxm + cxp + cym + cyp + czm + czp) * x[c] * L.inv_dx2;
+        }
+        r[c] = b[c] - ax;
+    }
+}
+
+int mf3d_apply_A(const mf3d_grid* g, const mf3d_bc* bc, int pin, const double* K, const double* x, double* y,
+                 void* stream) {
+    return guard([&] {
+        cudaStream_t s = (cudaStream_t)stream;
+        need(x, "x");
+        need(y, "y");
+        OneLevel L(g, bc, pin, K, s);
+        apply_A_kernel<<<grid1d(L.G.n, 256), 256, 0, s>>>(L.op, x, y);
+        MF3D_LAUNCH_CK();
+        MF3D_CK(cudaStreamSynchronize(s));
+    });
+}
+
+int mf3d_residual(const mf3d_grid* g, const mf3d_bc* bc, int pin, const double* K, const double* x, const double* b,
+                  double* r, void* stream) {
+    return guard([&] {
+        cudaStream_t s = (cudaStream_t)stream;
+        need(x, "x");
+        need(b, "b");
+        need(r, "r");
+        OneLevel L(g, bc, pin, K, s);
+        residual_mg_kernel<<<grid1d(L.G.n, 256), 256, 0, s>>>(L.op, x, b, r);
+        MF3D_LAUNCH_CK();
+        MF3D_CK(cudaStreamSynchronize(s));
+    });
+}
+
+int mf3d_gsrb(const mf3d_grid* g, const mf3d_bc* bc, int pin, const double* K, const double* b, double* x, int iters,
+              void* stream) {
+    return guard([&] {
+        cudaStream_t s = (cudaStream_t)stream;
+        need(b, "b");
+        need(x, "x");
+        if (iters < 0) throw Error(MF3D_E_INVALID, "iters < 0");
+        for (int a = 0; a < 3; ++a) {
+            const int n = a == 0 ? g->nx : (a == 1 ? g->ny : g->nz);
+            if (bc && bc->type[2 * a] == MF3D_BC_PERIODIC && (n & 1))
+                throw Error(MF3D_E_INVALID, "red-black smoothing needs an even cell count on a periodic axis");
+        }
+        OneLevel L(g, bc, pin, K, s);
+        if (iters == 0) return;
+        DevMem tmp(L.G.n * sizeof(double));
+        const int gx = (g->nx + SW_TX - 1) / SW_TX, gy = (g->ny + SW_TY - 1) / SW_TY;
+        const int zc = std::max(2, std::min(64, ((g->nz + 1) & ~1)));
+        dim3 grid(gx, gy, (g->nz + zc - 1) / zc);
+        double* bufs[2] = {x, tmp.as<double>()};
+        int cur = 0;
+        for (int it = 0; it < iters; ++it) {
+            SweepArgs<double, double, double> a{};
+            a.L = L.op;
+            a.b = b;
+            a.x_in = bufs[cur];
+            a.x_out = bufs[cur ^ 1];
+            a.zchunk = zc;
+            sweep_kernel<double, double, double, 0><<<grid, SW_NT, 0, s>>>(a);
+            MF3D_LAUNCH_CK();
+            cur ^= 1;
+        }
+        if (cur != 0) MF3D_CK(cudaMemcpyAsync(x, bufs[cur], L.G.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        MF3D_CK(cudaStreamSynchronize(s));
+    });
+}
+
+int mf3d_restrict(const mf3d_grid* c, const double* rf, double* bc_out, void* stream) {
+    return guard([&] {
+        check_grid(c);
+        need(rf, "r_fine");
+        need(bc_out, "b_coarse");
+        cudaStream_t s = (cudaStream_t)stream;
+        const size_t n = (size_t)c->nx * c->ny * c->nz;
+        restrict_kernel<double, double><<<grid1d(n, 256), 256, 0, s>>>(c->nx, c->ny, c->nz, rf, bc_out);
+        MF3D_LAUNCH_CK();
+        MF3D_CK(cudaStreamSynchronize(s));
+    });
+}
+
+int mf3d_prolong_add(const mf3d_grid* c, const double* xc, double* xf, void* stream) {
+    return guard([&] {
+        check_grid(c);
+        need(xc, "x_coarse");
+        need(xf, "x_fine");
+        cudaStream_t s = (cudaStream_t)stream;
+        const size_t nf = (size_t)8 * c->nx * c->ny * c->nz;
+        prolong_kernel<double><<<grid1d(nf, 256), 256, 0, s>>>(2 * c->nx, 2 * c->ny, 2 * c->nz, xf, xc, xf);
+        MF3D_LAUNCH_CK();
+        MF3D_CK(cudaStreamSynchronize(s));
+    });
+}
+
+int mf3d_coarsen_K(const mf3d_grid* c, const double* Kf, double* Kc, void* stream) {
+    return guard([&] {
+        check_grid(c);
+        need(Kf, "K_fine");
+        need(Kc, "K_coarse");
+        cudaStream_t s = (cudaStream_t)stream;
+        const size_t n = (size_t)c->nx * c->ny * c->nz;
+        coarsen_kernel<<<grid1d(n, 256), 256, 0, s>>>(c->nx, c->ny, c->nz, Kf, Kc);
+        MF3D_LAUNCH_CK();
+        MF3D_CK(cudaStreamSynchronize(s));
+    });
+}
+
+int mf3d_build_rhs(const mf3d_grid* g, const mf3d_bc* bc, const double* K, double* b, void* stream) {
+    return guard([&] {
+        check_grid(g);
+        need(bc, "bc");
+        need(K, "K");
+        need(b, "b");
+        cudaStream_t s = (cudaStream_t)stream;
+        const size_t n = (size_t)g->nx * g->ny * g->nz;
+        rhs_guess_kernel<<<grid1d(n, 256), 256, 0, s>>>(g->nx, g->ny, g->nz, g->dx, K, to_dev(*bc), b, nullptr);
+        MF3D_LAUNCH_CK();
+        MF3D_CK(cudaStreamSynchronize(s));
+    });
+}
+
+__global__ void guess_kernel(int nx, int ny, int nz, BcDev bc, double* __restrict__ h) {
+    const size_t n = (size_t)nx * ny * nz;
+    const bool lin = bc.type[0] == BC_DIRICHLET && bc.type[1] == BC_DIRICHLET;
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c % nx);
+        h[c] = lin ? bc.value[0] + (bc.value[1] - bc.value[0]) * (((double)i + 0.5) / (double)nx) : 0.0;
+    }
+}
+
+int mf3d_init_head_guess(const mf3d_grid* g, const mf3d_bc* bc, double* h, void* stream) {
+    return guard([&] {
+        check_grid(g);
+        need(bc, "bc");
+        need(h, "h");
+        cudaStream_t s = (cudaStream_t)stream;
+        const size_t n = (size_t)g->nx * g->ny * g->nz;
+        guess_kernel<<<grid1d(n, 256), 256, 0, s>>>(g->nx, g->ny, g->nz, to_dev(*bc), h);
+        MF3D_LAUNCH_CK();
+        MF3D_CK(cudaStreamSynchronize(s));
+    });
+}
+
+int mf3d_kfield_modes(unsigned long long seed, int n_modes, int cov, double lx, double ly, double lz,
+                      double* modes) {
+    return guard([&] {
+        need(modes, "modes_host");
+        if (n_modes <= 0) throw Error(MF3D_E_INVALID, "n_modes must be positive");
+        if (!(lx > 0 && ly > 0 && lz > 0)) throw Error(MF3D_E_INVALID, "correlation lengths must be positive");
+        if (cov != MF3D_COV_EXPONENTIAL && cov != MF3D_COV_GAUSSIAN) throw Error(MF3D_E_INVALID, "unknown covariance");
+        const double PI = 3.14159265358979323846;
+        double* k1 = modes;
+        double* k2 = modes + n_modes;
+        double* k3 = modes + 2 * (size_t)n_modes;
+        double* a = modes + 3 * (size_t)n_modes;
+        double* b = modes + 4 * (size_t)n_modes;
+        for (int m = 0; m < n_modes; ++m) {
+            ModeRng g{seed, (uint32_t)m};
+            // direction uniform on the sphere
+            const double fi = 2.0 * PI * g.next();
+            const double theta = std::acos(1.0 - 2.0 * g.next());
+            double k = 0.0;
+            if (cov == MF3D_COV_EXPONENTIAL) {
+                // radial density k^2/(1+k^2)^2 (3-D spectrum of exp(-r)): half-Cauchy proposal,
+                // accept with probability k^2/(1+k^2) (stochastic.cu:70-83)
+                for (int tries = 0; tries < 100000; ++tries) {
+                    k = std::tan(PI * 0.5 * g.next());
+                    if (g.next() < k * k / (1.0 + k * k)) break;
+                }
+            } else {
+                // radial density k^2 exp(-k^2/2) on [0, 10] by rejection, then scaled by sqrt(2)
+                // so that E cos(k.r) = exp(-r^2) (stochastic.cu:118-160)
+                for (int tries = 0; tries < 100000; ++tries) {
+                    k = 10.0 * g.next();
+                    if (g.next() * 2.0 * std::exp(-1.0) < k * k * std::exp(-0.5 * k * k)) break;
+                }
+                k *= std::sqrt(2.0);
+            }
+            k1[m] = k * std::sin(fi) * std::sin(theta) / lx;
+            k2[m] = k * std::cos(fi) * std::sin(theta) / ly;
+            k3[m] = k * std::cos(theta) / lz;
+            double u1 = g.next(), u2 = g.next();
+            a[m] = std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * PI * u2);
+            u1 = g.next();
+            u2 = g.next();
+            b[m] = std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * PI * u2);
+        }
+    });
+}
+
+int mf3d_kfield_eval(const mf3d_grid* g, int n_modes, const double* modes, double sigma2, double log_kg,
+                     int want_exp, double* out, void* stream) {
+    return guard([&] {
+        check_grid(g);
+        need(modes, "modes");
+        need(out, "out");
+        if (n_modes <= 0 || sigma2 < 0) throw Error(MF3D_E_INVALID, "bad n_modes or variance");
+        cudaStream_t s = (cudaStream_t)stream;
+        const size_t tasks = (size_t)g->ny * g->nz * ((g->nx + KF_SEG - 1) / KF_SEG);
+        kfield_kernel<<<(unsigned)((tasks + KF_NT - 1) / KF_NT), KF_NT, 0, s>>>(
+            g->nx, g->ny, g->nz, g->dx, n_modes, modes, std::sqrt(sigma2), log_kg, want_exp, out);
+        MF3D_LAUNCH_CK();
+        MF3D_CK(cudaStreamSynchronize(s));
+    });
+}
+
+} // extern "C"

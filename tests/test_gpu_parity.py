@@ -1,0 +1,252 @@
+"""GPU parity: the CUDA path (through the C-ABI) against the CPU oracle on seeded inputs.
+
+Tolerances: single operator applications are compared element-wise at 1e-12 relative to
+the array's max (the arithmetic differs only in rounding: stored vs recomputed harmonic
+means, operation order, FMA); solves are compared by head relative max-norm <= 1e-9 and
+mass balance <= 1e-10, the targets of the task statement for this path.
+"""
+import zlib
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+D, N, P = 0, 1, 2
+BC_CASES = [
+    ("darcy", [D, D, N, N, N, N], [1.0, 0.0, 0, 0, 0, 0], False),
+    ("mixed", [D, N, N, D, N, D], [1.0, 0, 0, 0.5, 0, 0.25], False),
+    ("neumann_pin", [N, N, N, N, N, N], [0.0] * 6, True),
+    ("periodic", [P, P, N, N, D, D], [0, 0, 0, 0, 0.3, 0.7], False),
+    ("all_dirichlet", [D] * 6, [1.0, 0.0, 0.2, 0.4, 0.6, 0.8], False),
+]
+SHAPES = [(8, 10, 6), (6, 8, 12), (12, 34, 40), (16, 16, 16)]
+
+
+def _t(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).cuda()
+
+
+def _np(t):
+    return t.detach().cpu().numpy()
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def _bcs(M, types, values):
+    return M.BCSpec([M.BCFace(t, v) for t, v in zip(types, values)])
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("case", BC_CASES, ids=[c[0] for c in BC_CASES])
+def test_operators_vs_oracle(mf3d, oracle_mod, shape, case):
+    M, O = mf3d, oracle_mod
+    name, types, values, pin = case
+    rng = np.random.default_rng(zlib.crc32(repr((shape, name)).encode()))
+    K = np.exp(rng.normal(size=shape))
+    x, b = rng.normal(size=shape), rng.normal(size=shape)
+    dx = 0.5
+    g = M.Grid3D(shape[2], shape[1], shape[0], dx)
+    bc, obc = _bcs(M, types, values), O.make_bc(types, values)
+    Kt, xt, bt = _t(K), _t(x), _t(b)
+    y = _t(np.zeros(shape))
+    M.apply_A(g, bc, Kt, xt, y, pin)
+    assert _rel(_np(y), O.apply_A(K, x, obc, dx, pin)) < 1e-12
+    M.compute_residual_3d(g, xt, bt, Kt, y, bc, pin)
+    assert _rel(_np(y), O.residual(K, x, b, obc, dx, pin)) < 1e-12
+    for it in (1, 3):
+        xs = xt.clone()
+        M.gsrb_smooth_3d(g, xs, bt, Kt, it, bc, pin)
+        assert _rel(_np(xs), O.gsrb(K, b, x, obc, it, dx, pin)) < 1e-11, it
+    M.build_rhs_head(y, Kt, g, bc)
+    assert _rel(_np(y), O.build_rhs(K, obc, dx)) < 1e-14 or np.abs(O.build_rhs(K, obc, dx)).max() == 0
+    M.init_head_guess(y, g, bc)
+    assert np.abs(_np(y) - O.init_guess(shape, obc)).max() < 1e-15
+    for lay in (0, 1):
+        su, sv, sw = M.velocity_sizes(g, lay)
+        U, V, W = _t(np.zeros(su)), _t(np.zeros(sv)), _t(np.zeros(sw))
+        M.compute_velocity_from_head(U, V, W, xt, Kt, g, bc, lay)
+        Uo, Vo, Wo = O.velocity(x, K, obc, dx, lay)
+        for a, o in ((U, Uo), (V, Vo), (W, Wo)):
+            assert np.abs(_np(a) - o.ravel()).max() <= 1e-14 * np.abs(o).max()
+
+
+def test_transfer_vs_oracle(mf3d, oracle_mod):
+    M, O = mf3d, oracle_mod
+    rng = np.random.default_rng(5)
+    fine = rng.normal(size=(8, 12, 16))
+    coarse = rng.normal(size=(4, 6, 8))
+    Kf = np.exp(rng.normal(size=(8, 12, 16)))
+    cg = M.Grid3D(8, 6, 4, 2.0)
+    out = _t(np.zeros((4, 6, 8)))
+    M.restrict_3d(cg, _t(fine), out)
+    assert _rel(_np(out), O.restrict(fine)) < 1e-15
+    xf = _t(fine)
+    M.prolong_3d_add(cg, _t(coarse), xf)
+    assert _rel(_np(xf), O.prolong_add(coarse, fine)) < 1e-15
+    M.coarsen_K(cg, _t(Kf), out)
+    assert _rel(_np(out), O.coarsen_K(Kf)) < 1e-14
+
+
+@pytest.mark.parametrize("shape,levels,pre,post,coarse", [
+    ((16, 16, 16), 3, 2, 2, 50), ((32, 32, 32), 4, 2, 2, 50), ((64, 32, 32), 4, 1, 3, 20),
+    ((8, 8, 8), 2, 2, 2, 50), ((64, 64, 64), 5, 2, 2, 50)])
+@pytest.mark.parametrize("case", BC_CASES[:4], ids=[c[0] for c in BC_CASES[:4]])
+def test_vcycle_vs_oracle(mf3d, oracle_mod, shape, levels, pre, post, coarse, case):
+    M, O = mf3d, oracle_mod
+    name, types, values, pin = case
+    rng = np.random.default_rng(zlib.crc32(repr((shape, name, 1)).encode()))
+    K = np.exp(rng.normal(size=shape))
+    r = rng.normal(size=shape)
+    g = M.Grid3D(shape[2], shape[1], shape[0], 1.0)
+    cfg = M.HeadSolveConfig(mg_levels=levels, mg_pre_smooth=pre, mg_post_smooth=post,
+                            mg_coarse_iters=coarse, pin_mode=M.PIN_ON if pin else M.PIN_OFF)
+    s = M.HeadSolver(g, _bcs(M, types, values), cfg)
+    s.set_K(_t(K))
+    z = _t(np.zeros(shape))
+    s.vcycle(_t(r), z)
+    zo, nl = O.vcycle(K, r, O.make_bc(types, values), levels, pre, post, coarse, 1.0, pin)
+    assert nl == s.num_levels
+    assert _rel(_np(z), zo) < 1e-10
+
+
+def _lognormal(shape, sigma, seed):
+    return np.exp(sigma * np.random.default_rng(seed).normal(size=shape))
+
+
+@pytest.mark.parametrize("shape,sigma,levels", [((16, 16, 16), 1.0, 3), ((24, 40, 32), 2.0, 4),
+                                                ((64, 64, 64), 1.0, 5)])
+def test_pcg_reference_semantics_vs_oracle(mf3d, oracle_mod, shape, sigma, levels):
+    """Reference stopping rule (||r||/||r0|| < rtol every check_every): same iteration count."""
+    M, O = mf3d, oracle_mod
+    K = _lognormal(shape, sigma, 11)
+    g = M.Grid3D(shape[2], shape[1], shape[0], 1.0)
+    bc = M.BCSpec.darcy_x()
+    cfg = M.HeadSolveConfig(mg_levels=levels, cg_rtol=1e-10, cg_check_every=1)
+    s = M.HeadSolver(g, bc, cfg)
+    s.set_K(_t(K))
+    h = _t(np.zeros(shape))
+    res = s.solve(h)
+    ho, ro = O.solve_head_pcg(K, O.baseline_bc(), levels, rtol=1e-10, check_every=1)
+    assert res.converged and ro.converged
+    assert abs(res.num_iterations - ro.iterations) <= 1
+    assert _rel(_np(h), ho) < 1e-9
+    assert res.true_rel_residual < 1e-9
+
+
+@pytest.mark.parametrize("prec", [0, 1, 2])
+def test_mixed_precision_reaches_fp64_tolerance(mf3d, oracle_mod, prec):
+    """FP32 / BF16-coefficient V-cycle inside flexible FP64 PCG to ||r||/||b|| <= 1e-10;
+    the head agrees with a tightly solved FP64 oracle head."""
+    M, O = mf3d, oracle_mod
+    shape = (32, 32, 32)
+    K = _lognormal(shape, 2.0, 12)
+    g = M.Grid3D(32, 32, 32, 1.0)
+    cfg = M.HeadSolveConfig(mg_levels=4, cg_rtol=1e-10, cg_check_every=1, conv_norm=M.CONV_B,
+                            precision=prec)
+    s = M.HeadSolver(g, M.BCSpec.darcy_x(), cfg)
+    s.set_K(_t(K))
+    h = _t(np.zeros(shape))
+    res = s.solve(h)
+    assert res.converged, res
+    assert res.true_rel_residual <= 1.5e-10
+    ho, _ = O.solve_head_pcg(K, O.baseline_bc(), 4, rtol=1e-13, check_every=1)
+    assert _rel(_np(h), ho) < 1e-7
+
+
+def test_graph_and_host_loop_identical(mf3d):
+    M = mf3d
+    shape = (32, 32, 32)
+    K = _t(_lognormal(shape, 1.5, 13))
+    g = M.Grid3D(32, 32, 32, 1.0)
+    out = []
+    for ug in (1, 0):
+        cfg = M.HeadSolveConfig(mg_levels=4, cg_rtol=1e-10, cg_check_every=1, use_graph=ug)
+        s = M.HeadSolver(g, M.BCSpec.darcy_x(), cfg)
+        s.set_K(K)
+        h = _t(np.zeros(shape))
+        r = s.solve(h)
+        out.append((r.num_iterations, _np(h)))
+    assert out[0][0] == out[1][0]
+    assert np.array_equal(out[0][1], out[1][1])  # deterministic reductions: bitwise equal
+
+
+def test_repeated_solves_deterministic(mf3d):
+    M = mf3d
+    shape = (32, 32, 64)
+    K = _t(_lognormal(shape, 1.0, 14))
+    g = M.Grid3D(64, 32, 32, 1.0)
+    s = M.HeadSolver(g, M.BCSpec.darcy_x(), M.HeadSolveConfig(mg_levels=4, cg_rtol=1e-10))
+    s.set_K(K)
+    hs = []
+    for _ in range(3):
+        h = _t(np.zeros(shape))
+        s.solve(h)
+        hs.append(_np(h))
+    assert np.array_equal(hs[0], hs[1]) and np.array_equal(hs[1], hs[2])
+
+
+def test_velocity_mass_balance_after_solve(mf3d, oracle_mod):
+    M, O = mf3d, oracle_mod
+    shape = (32, 32, 32)
+    K = _lognormal(shape, 1.0, 15)
+    g = M.Grid3D(32, 32, 32, 1.0)
+    bc = M.BCSpec.darcy_x()
+    s = M.HeadSolver(g, bc, M.HeadSolveConfig(mg_levels=4, cg_rtol=1e-12, cg_check_every=1,
+                                              conv_norm=M.CONV_B))
+    Kt = _t(K)
+    s.set_K(Kt)
+    h = _t(np.zeros(shape))
+    s.solve(h)
+    su, sv, sw = M.velocity_sizes(g)
+    U, V, W = _t(np.zeros(su)), _t(np.zeros(sv)), _t(np.zeros(sw))
+    mx, qin, qout = M.velocity_mass_balance(U, V, W, h, Kt, g, bc)
+    assert mx / abs(qin) < 1e-10 and abs(qin - qout) / abs(qin) < 1e-10
+    Uo, _, _ = O.velocity(_np(h), K, O.baseline_bc())
+    assert _rel(_np(U), Uo.ravel()) < 1e-14
+
+
+def test_warm_start_and_nonconvergence_reporting(mf3d):
+    M = mf3d
+    shape = (32, 32, 32)
+    K = _t(_lognormal(shape, 1.0, 16))
+    g = M.Grid3D(32, 32, 32, 1.0)
+    s = M.HeadSolver(g, M.BCSpec.darcy_x(), M.HeadSolveConfig(mg_levels=4, cg_rtol=1e-10,
+                                                              cg_check_every=1, conv_norm=M.CONV_B))
+    s.set_K(K)
+    h = _t(np.zeros(shape))
+    r1 = s.solve(h)
+    h2 = _t(np.zeros(shape))
+    r2 = s.solve(h2, x0=h)  # warm start from the converged head
+    assert r2.num_iterations <= 1 and r2.converged
+    s3 = M.HeadSolver(g, M.BCSpec.darcy_x(), M.HeadSolveConfig(mg_levels=4, cg_rtol=1e-14,
+                                                               cg_max_iter=3, cg_check_every=1))
+    s3.set_K(K)
+    r3 = s3.solve(h2)
+    assert not r3.converged and r3.num_iterations == 3 and r1.converged
+
+
+def test_nonfinite_K_reports_status(mf3d):
+    M = mf3d
+    shape = (16, 16, 16)
+    Kn = _lognormal(shape, 1.0, 17)
+    Kn[3, 4, 5] = np.nan
+    g = M.Grid3D(16, 16, 16, 1.0)
+    s = M.HeadSolver(g, M.BCSpec.darcy_x(), M.HeadSolveConfig(mg_levels=3, cg_rtol=1e-10))
+    s.set_K(_t(Kn))
+    res = s.solve(_t(np.zeros(shape)))
+    assert not res.converged and res.status == 2
+
+
+def test_kfield_vs_oracle(mf3d, oracle_mod):
+    M, O = mf3d, oracle_mod
+    g = M.Grid3D(37, 9, 5, 1.0)
+    modes = M.kfield_modes(99, 1000, M.COV_EXPONENTIAL, (4.0, 4.0, 2.0))
+    lnk = M.generate_K_field(g, 2.0, (4.0, 4.0, 2.0), seed=99, log_only=True)
+    ref = O.lnk_eval((5, 9, 37), modes, np.sqrt(2.0))
+    assert np.abs(_np(lnk) - ref).max() < 1e-9
+    K = M.generate_K_field(g, 2.0, (4.0, 4.0, 2.0), seed=99)
+    assert np.allclose(_np(K), np.exp(ref), rtol=1e-9)
