@@ -108,10 +108,13 @@ def levels_for(n):
     return lv
 
 
+USE_GRAPH = 1
+
+
 def solver_cfg(M, n, precision, rtol=1e-10):
     return M.HeadSolveConfig(mg_levels=levels_for(n), mg_pre_smooth=2, mg_post_smooth=2,
                              mg_coarse_iters=50, cg_max_iter=500, cg_check_every=1, cg_rtol=rtol,
-                             conv_norm=M.CONV_B, precision=precision)
+                             conv_norm=M.CONV_B, precision=precision, use_graph=USE_GRAPH)
 
 
 def run_steps(M, n, K, precision, steps, warmup, dist_ctx=None):
@@ -257,7 +260,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--profile-kernels", action="store_true", help="print per-kernel timings")
     ap.add_argument("--seed", type=int, default=20240601)
+    ap.add_argument("--no-graph", action="store_true",
+                    help="host-driven PCG loop instead of the CUDA-graph while loop (for profilers)")
     args = ap.parse_args()
+    global USE_GRAPH
+    USE_GRAPH = 0 if args.no_graph else 1
     args.warmup = max(args.warmup, 3)
 
     import torch
@@ -317,7 +324,7 @@ def main():
             "data": "synthetic (seeded randomization-method lnK field)", "config": config}
     line["iterations"] = out["iters"][-1]
     line["true_rel_residual"] = res.true_rel_residual
-    line["cell_updates_per_s"] = round(n ** 3 * out["iters"][-1] * value / world * world, 1)
+    line["cell_updates_per_s"] = round(n ** 3 * out["iters"][-1] * value, 1)
     line["gpu_launches"] = out["launches"] * args.steps
     line["clocks"] = clocks
 

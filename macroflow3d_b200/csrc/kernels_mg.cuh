@@ -33,9 +33,10 @@ template <class T, class TC, class TB> struct SweepArgs {
     int ncx, ncy;
     T* b_coarse;       // restricted residual (M_RESID)
     int zchunk;        // planes per CTA (even)
-    double* dot_partials; // M_DOT: <b, x_out> summed over the grid into *dot_out
+    double* dot_partials; // M_DOT: <r64, x_out> summed over the grid into *dot_out
     unsigned* dot_ticket;
     double* dot_out;
+    const double* r64;    // FP64 residual for M_DOT
 };
 
 __device__ __forceinline__ int pmod(int a, int m) {
@@ -152,7 +153,7 @@ __global__ void __launch_bounds__(SW_NT) sweep_kernel(const SweepArgs<T, TC, TB>
                     const size_t c = (size_t)gi + (size_t)nx * gj + nxy * q;
                     const T v = xs[sl][lj + H][li + H];
                     a.x_out[c] = v;
-                    if (DOT) dot_acc += load_as<double>(a.b, c) * (double)v;
+                    if (DOT) dot_acc += __ldg(a.r64 + c) * (double)v;
                 }
             }
         }
@@ -248,142 +249,6 @@ __global__ void restrict_kernel(int ncx, int ncy, int ncz, const TB* fine, T* co
         acc += (T)fine[f + nxy + nx + 1];
         coarse[C] = acc / (T)8;
     }
-}
-
-// ---------------------------------------------------------------------------------------
-// Coarse tail: the V-cycle below (and including) level `first` in ONE CTA, in FP64, with
-// x and b of every tail level held in shared memory and GSRB done in place (one colour
-// per phase, __syncthreads between phases) exactly as gsrb_smooth_3d / v_cycle_recursive
-// order it (src/multigrid/cycle/v_cycle.cu:36-74).  The coarsest level's 50 sweeps run
-// on warp 0 alone when it has <= 64 cells per lane, with warp barriers.
-// ---------------------------------------------------------------------------------------
-constexpr int TAIL_MAX_LEVELS = 8;
-constexpr int TAIL_NT = 1024;
-
-struct TailArgs {
-    int nlev;
-    LevelOp<double> L[TAIL_MAX_LEVELS];
-    int off[TAIL_MAX_LEVELS]; // offsets (in doubles) of each level's x / b in shared memory
-    int pre, post, coarse_iters;
-};
-
-__device__ __forceinline__ double tail_nb(const double* x, const LevelOp<double>& L, int i, int j, int k,
-                                          size_t c, int dir) {
-    // neighbour value in shared memory (0 outside a non-periodic boundary)
-    const size_t nxy = (size_t)L.nx * L.ny;
-    switch (dir) {
-    case 0: return i > 0 ? x[c - 1] : (L.per_x ? x[c + L.nx - 1] : 0.0);
-    case 1: return i < L.nx - 1 ? x[c + 1] : (L.per_x ? x[c - (L.nx - 1)] : 0.0);
-    case 2: return j > 0 ? x[c - L.nx] : (L.per_y ? x[c + (size_t)(L.ny - 1) * L.nx] : 0.0);
-    case 3: return j < L.ny - 1 ? x[c + L.nx] : (L.per_y ? x[c - (size_t)(L.ny - 1) * L.nx] : 0.0);
-    case 4: return k > 0 ? x[c - nxy] : (L.per_z ? x[c + (size_t)(L.nz - 1) * nxy] : 0.0);
-    default: return k < L.nz - 1 ? x[c + nxy] : (L.per_z ? x[c - (size_t)(L.nz - 1) * nxy] : 0.0);
-    }
-}
-
-__device__ __forceinline__ double tail_relax(const double* x, const double* b, const LevelOp<double>& L,
-                                             int i, int j, int k, size_t c) {
-    double cxm, cxp, cym, cyp, czm, czp;
-    cell_coefs<double>(L, i, j, k, c, cxm, cxp, cym, cyp, czm, czp);
-    double D = cxm + cxp + cym + cyp + czm + czp;
-    if (L.pin && c == 0) D *= 2.0;
-    const double s = cxp * tail_nb(x, L, i, j, k, c, 1) + cxm * tail_nb(x, L, i, j, k, c, 0) +
-                     cyp * tail_nb(x, L, i, j, k, c, 3) + cym * tail_nb(x, L, i, j, k, c, 2) +
-                     czp * tail_nb(x, L, i, j, k, c, 5) + czm * tail_nb(x, L, i, j, k, c, 4);
-    return (s - b[c] * L.dx2) / D;
-}
-
-// `sweeps` GSRB sweeps on one tail level, threads [0, nthr) participating.
-__device__ __forceinline__ void tail_gsrb(double* x, const double* b, const LevelOp<double>& L,
-                                          int sweeps, bool warp_only) {
-    const int n = L.nx * L.ny * L.nz;
-    const int nthr = warp_only ? 32 : TAIL_NT;
-    const int tid = threadIdx.x;
-    if (warp_only && tid >= 32) return;
-    for (int it = 0; it < sweeps; ++it)
-        for (int color = 0; color < 2; ++color) {
-            for (int c = tid; c < n; c += nthr) {
-                const int i = c % L.nx, j = (c / L.nx) % L.ny, k = c / (L.nx * L.ny);
-                if (((i + j + k) & 1) != color) continue;
-                x[c] = tail_relax(x, b, L, i, j, k, c);
-            }
-            if (warp_only) __syncwarp();
-            else __syncthreads();
-        }
-}
-
-template <class TI, class TO>
-__global__ void __launch_bounds__(TAIL_NT, 1) tail_kernel(const TailArgs a, const TI* b_in, TO* x_out) {
-    extern __shared__ double sm[];
-    const int tid = threadIdx.x;
-    const LevelOp<double>& L0 = a.L[0];
-    const int n0 = L0.nx * L0.ny * L0.nz;
-    // load b of the top tail level, zero every x
-    for (int c = tid; c < n0; c += TAIL_NT) {
-        sm[a.off[0] + n0 + c] = (double)b_in[c];
-    }
-    for (int l = 0; l < a.nlev; ++l) {
-        const int n = a.L[l].nx * a.L[l].ny * a.L[l].nz;
-        for (int c = tid; c < n; c += TAIL_NT) sm[a.off[l] + c] = 0.0;
-    }
-    __syncthreads();
-    // down: pre-smooth, residual + restriction
-    for (int l = 0; l + 1 < a.nlev; ++l) {
-        const LevelOp<double>& L = a.L[l];
-        double* x = sm + a.off[l];
-        const int n = L.nx * L.ny * L.nz;
-        double* b = x + n;
-        tail_gsrb(x, b, L, a.pre, false);
-        const LevelOp<double>& Lc = a.L[l + 1];
-        const int nc = Lc.nx * Lc.ny * Lc.nz;
-        double* bc = sm + a.off[l + 1] + nc;
-        for (int C = tid; C < nc; C += TAIL_NT) {
-            const int I = C % Lc.nx, J = (C / Lc.nx) % Lc.ny, K = C / (Lc.nx * Lc.ny);
-            double acc = 0.0;
-            // children in the order (000,100,010,110,001,101,011,111)
-            for (int dz = 0; dz < 2; ++dz)
-                for (int dy = 0; dy < 2; ++dy)
-                    for (int dxx = 0; dxx < 2; ++dxx) {
-                        const int i = 2 * I + dxx, j = 2 * J + dy, k = 2 * K + dz;
-                        const size_t c = (size_t)i + (size_t)L.nx * (j + (size_t)L.ny * k);
-                        double cxm, cxp, cym, cyp, czm, czp;
-                        cell_coefs<double>(L, i, j, k, c, cxm, cxp, cym, cyp, czm, czp);
-                        double D = cxm + cxp + cym + cyp + czm + czp;
-                        if (L.pin && c == 0) D *= 2.0;
-                        const double s = cxp * tail_nb(x, L, i, j, k, c, 1) + cxm * tail_nb(x, L, i, j, k, c, 0) +
-                                         cyp * tail_nb(x, L, i, j, k, c, 3) + cym * tail_nb(x, L, i, j, k, c, 2) +
-                                         czp * tail_nb(x, L, i, j, k, c, 5) + czm * tail_nb(x, L, i, j, k, c, 4);
-                        acc += b[c] - (s - D * x[c]) * L.inv_dx2;
-                    }
-            bc[C] = acc / 8.0;
-        }
-        __syncthreads();
-    }
-    // coarsest
-    {
-        const int l = a.nlev - 1;
-        const LevelOp<double>& L = a.L[l];
-        double* x = sm + a.off[l];
-        const int n = L.nx * L.ny * L.nz;
-        const bool warp_only = n <= 64 * 32;
-        tail_gsrb(x, x + n, L, a.coarse_iters, warp_only);
-        __syncthreads();
-    }
-    // up: prolongation + post-smooth
-    for (int l = a.nlev - 2; l >= 0; --l) {
-        const LevelOp<double>& L = a.L[l];
-        const LevelOp<double>& Lc = a.L[l + 1];
-        double* x = sm + a.off[l];
-        const double* xc = sm + a.off[l + 1];
-        const int n = L.nx * L.ny * L.nz;
-        for (int c = tid; c < n; c += TAIL_NT) {
-            const int i = c % L.nx, j = (c / L.nx) % L.ny, k = c / (L.nx * L.ny);
-            x[c] += xc[(i >> 1) + Lc.nx * ((j >> 1) + Lc.ny * (k >> 1))];
-        }
-        __syncthreads();
-        tail_gsrb(x, x + n, L, a.post, false);
-    }
-    for (int c = tid; c < n0; c += TAIL_NT) x_out[c] = (TO)sm[a.off[0] + c];
 }
 
 } // namespace mf3d

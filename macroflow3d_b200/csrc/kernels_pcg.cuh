@@ -68,7 +68,7 @@ template <class TC>
 __global__ void __launch_bounds__(PK_NT) residual_kernel(const LevelOp<TC> L, const double* __restrict__ x,
                                                          const double* __restrict__ b, double* __restrict__ r,
                                                          PcgState* st, double* partials, unsigned* ticket,
-                                                         int mode, int ref_is_b) {
+                                                         int mode, int ref_is_b, float* __restrict__ r32) {
     const size_t n = (size_t)L.nx * L.ny * L.nz;
     double srr = 0.0, sbb = 0.0;
     for (size_t c = blockIdx.x * (size_t)PK_NT + threadIdx.x; c < n; c += (size_t)gridDim.x * PK_NT) {
@@ -76,6 +76,7 @@ __global__ void __launch_bounds__(PK_NT) residual_kernel(const LevelOp<TC> L, co
         const double bv = b[c];
         const double rv = bv + (-1.0) * apply_A_cell(L, x, i, j, k, c);
         r[c] = rv;
+        if (r32) r32[c] = (float)rv;
         srr += rv * rv;
         sbb += bv * bv;
     }
@@ -142,7 +143,8 @@ __global__ void __launch_bounds__(PK_NT) xr_update_kernel(size_t n, double* __re
                                                           double* __restrict__ r, const double* __restrict__ Ap,
                                                           const TZ* __restrict__ z, PcgState* st,
                                                           double* partials, unsigned* ticket,
-                                                          cudaGraphConditionalHandle cond, int use_cond) {
+                                                          cudaGraphConditionalHandle cond, int use_cond,
+                                                          float* __restrict__ r32) {
     const PcgState s = *st;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         // Loop bound that does not depend on the reductions: a body count and a device-time
@@ -165,6 +167,7 @@ __global__ void __launch_bounds__(PK_NT) xr_update_kernel(size_t n, double* __re
         x[c] = x[c] + alpha * p[c];
         const double rv = r[c] + (-alpha) * Ap[c];
         r[c] = rv;
+        if (r32) r32[c] = (float)rv;
         srr += rv * rv;
         if (s.flexible) sg += rv * (double)z[c];
     }
@@ -201,6 +204,15 @@ __global__ void __launch_bounds__(PK_NT) xr_update_kernel(size_t n, double* __re
 // Sets the while condition before the loop from the state left by residual_kernel(mode 0).
 __global__ void loop_gate_kernel(const PcgState* st, cudaGraphConditionalHandle cond) {
     cudaGraphSetConditional(cond, st->stop ? 0u : 1u);
+}
+
+// Re-opens a finished state so the iteration kernels can be timed in isolation (diagnostics).
+__global__ void pcg_reopen_kernel(PcgState* st) {
+    st->stop = 0;
+    st->body_count = 0;
+    st->iter = 1;
+    st->rtol = 0.0; // never converges while being timed
+    st->t_start_ns = global_ns();
 }
 
 // PCG state initialisation (host-given controls).

@@ -33,6 +33,13 @@ __device__ __forceinline__ float ld_as_float(double v) { return (float)v; }
 __device__ __forceinline__ float ld_as_float(float v) { return v; }
 __device__ __forceinline__ float ld_as_float(__nv_bfloat16 v) { return __bfloat162float(v); }
 
+// value of a stored coefficient (double, float or bf16) as the compute type T
+template <class T> __device__ __forceinline__ T ld_as_float_or_double(double v) { return (T)v; }
+template <class T> __device__ __forceinline__ T ld_as_float_or_double(float v) { return (T)v; }
+template <class T> __device__ __forceinline__ T ld_as_float_or_double(__nv_bfloat16 v) {
+    return (T)__bfloat162float(v);
+}
+
 template <class T> __device__ __forceinline__ T cvt(double v);
 template <> __device__ __forceinline__ double cvt<double>(double v) { return v; }
 template <> __device__ __forceinline__ float cvt<float>(double v) { return (float)v; }

@@ -10,7 +10,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -24,6 +26,8 @@
 #include "kernels_mg.cuh"
 #include "kernels_pcg.cuh"
 #include "kernels_setup.cuh"
+#include "kernels_sweep_tma.cuh"
+#include "kernels_tail.cuh"
 #include "kernels_velocity.cuh"
 
 namespace mf3d {
@@ -226,26 +230,70 @@ static mf3d_kernel_timing timing(const char* name, float ms, double bytes, int p
 struct VCycleBase {
     virtual ~VCycleBase() {}
     virtual void build_coefs(cudaStream_t s, const std::vector<const double*>& Klev) = 0;
-    // z (type T) = V-cycle(r); if rho_out != null, <r, z> is summed into *rho_out.
-    virtual void run(cudaStream_t s, const double* r, void* z, double* rho_out) = 0;
+    // z (type T) = V-cycle of the level-0 right-hand side bound at construction; when
+    // rho_out != null, <r64, z> is summed into *rho_out.
+    virtual void run(cudaStream_t s, void* z, double* rho_out) = 0;
     // per-kernel timings of one V-cycle (level-0 sweeps by role, the coarse tail, the whole cycle)
-    virtual void profile(Timer& tm, int reps, const double* r, void* z, double* rho_out,
-                         std::vector<mf3d_kernel_timing>& out) = 0;
+    virtual void profile(Timer& tm, int reps, void* z, double* rho_out, std::vector<mf3d_kernel_timing>& out) = 0;
     virtual size_t z_elt() const = 0;
     virtual size_t bytes() const = 0;
+    virtual int tma_levels() const = 0;
 };
 
 struct Scratch {
     double* partials;
     unsigned* tickets; // one per reduction site
     size_t partial_cap;
+    int* err;          // device error flag of the TMA pipelines
 };
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        MF3D_CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !p) throw Error(MF3D_E_CUDA, "cuTensorMapEncodeTiled unavailable");
+        fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+template <class E> static CUtensorMapDataType tma_dtype();
+template <> CUtensorMapDataType tma_dtype<double>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT64; }
+template <> CUtensorMapDataType tma_dtype<float>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT32; }
+template <> CUtensorMapDataType tma_dtype<__nv_bfloat16>() { return CU_TENSOR_MAP_DATA_TYPE_BFLOAT16; }
+
+// 3-D tiled map over an nx*ny*nz array, box bx*by*1; out-of-range elements read as zero.
+template <class E> static CUtensorMap make_map(const void* base, const Geom& g, int bx, int by) {
+    if (((uintptr_t)base & 15) || ((size_t)g.nx * sizeof(E)) % 16)
+        throw Error(MF3D_E_INVALID, "array not aligned for TMA");
+    CUtensorMap m;
+    cuuint64_t dims[3] = {(cuuint64_t)g.nx, (cuuint64_t)g.ny, (cuuint64_t)g.nz};
+    cuuint64_t strides[2] = {(cuuint64_t)g.nx * sizeof(E), (cuuint64_t)g.nx * g.ny * sizeof(E)};
+    cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1u};
+    cuuint32_t es[3] = {1u, 1u, 1u};
+    CUresult r = encode_fn()(&m, tma_dtype<E>(), 3, const_cast<void*>(base), dims, strides, box, es,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(MF3D_E_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return m;
+}
 
 template <class T, class TC> class VCycle : public VCycleBase {
   public:
+    // b0: level-0 right-hand side in the V-cycle's type (the PCG residual or its FP32 copy);
+    // r64: the FP64 residual (dot products, and the right-hand side when the whole V-cycle is
+    // the coarse tail).
     VCycle(const std::vector<Geom>& G, int Lt, const mf3d_bc& bc, bool pin, int pre, int post, int coarse,
-           const std::vector<LevelOp<double>>& op64, Scratch scr)
-        : G_(G), Lt_(Lt), bc_(bc), pin_(pin), pre_(pre), post_(post), coarse_(coarse), op64_(op64), scr_(scr) {
+           const std::vector<LevelOp<double>>& op64, Scratch scr, const T* b0, const double* r64, bool allow_tma)
+        : G_(G), Lt_(Lt), bc_(bc), pin_(pin), pre_(pre), post_(post), coarse_(coarse), op64_(op64), scr_(scr),
+          b0_(b0), r64_(r64) {
         const int nl = (int)G.size();
         ops_.resize(Lt);
         coef_.resize(Lt);
@@ -277,40 +325,86 @@ template <class T, class TC> class VCycle : public VCycleBase {
             bl_[l].reset(new DevMem(G[l].n * sizeof(T)));
             bytes_ += G[l].n * sizeof(T);
         }
-        // tail
+        // TMA tensor maps for every level the staged sweep can serve
+        tma_.assign(Lt, 0);
+        maps_.resize(Lt);
+        const bool periodic = bc.type[0] == MF3D_BC_PERIODIC || bc.type[2] == MF3D_BC_PERIODIC ||
+                              bc.type[4] == MF3D_BC_PERIODIC;
+        for (int l = 0; l < Lt && allow_tma && !periodic; ++l) {
+            const Geom& g = G[l];
+            if ((g.nx * sizeof(T)) % 16 || (g.nx * sizeof(TC)) % 16 || g.nx < 16 || g.ny < 8) continue;
+            tma_[l] = 1;
+            ++n_tma_;
+            for (int resid = 0; resid < 2; ++resid) {
+                const int H = resid ? 3 : 2;
+                const int bx = SW_TX + 2 * TmaGeom<T, TC>::hx(H), by = SW_TY + 2 * H;
+                Maps4& m = maps_[l][resid];
+                const T* b = l == 0 ? b0_ : (const T*)bl_[l]->p;
+                m.xa.x = make_map<T>(xa_[l]->p, g, bx, by);
+                m.xa.b = make_map<T>(b, g, bx, by);
+                m.xa.cx = make_map<TC>(ops_[l].cx, g, bx, by);
+                m.xa.cy = make_map<TC>(ops_[l].cy, g, bx, by);
+                m.xa.cz = make_map<TC>(ops_[l].cz, g, bx, by);
+                m.xb = m.xa;
+                m.xb.x = make_map<T>(xb_[l]->p, g, bx, by);
+            }
+        }
+        if (n_tma_) set_tma_smem();
+        // coarse tail: FP64 weights per cell, x (ghost-padded) and b in shared memory
         if (Lt < nl) {
             tail_.nlev = nl - Lt;
-            if (tail_.nlev > TAIL_MAX_LEVELS) throw Error(MF3D_E_INVALID, "too many coarse tail levels");
-            int off = 0;
-            for (int l = Lt; l < nl; ++l) {
-                tail_.L[l - Lt] = op64[l];
-                tail_.off[l - Lt] = off;
-                off += 2 * (int)G[l].n;
-            }
+            if (tail_.nlev > TAIL2_MAX_LEVELS) throw Error(MF3D_E_INVALID, "too many coarse tail levels");
             tail_.pre = pre;
             tail_.post = post;
             tail_.coarse_iters = coarse;
+            size_t wtot = 0;
+            for (int l = Lt; l < nl; ++l) wtot += 8 * G[l].n;
+            tail_w_.reset(new DevMem(wtot * sizeof(double)));
+            bytes_ += tail_w_->bytes;
+            int off = 0;
+            size_t woff = 0;
+            for (int l = Lt; l < nl; ++l) {
+                TailLevel& T2 = tail_.L[l - Lt];
+                T2.nx = G[l].nx;
+                T2.ny = G[l].ny;
+                T2.nz = G[l].nz;
+                T2.n = (int)G[l].n;
+                T2.per_x = op64[l].per_x;
+                T2.per_y = op64[l].per_y;
+                T2.per_z = op64[l].per_z;
+                T2.xoff = off;
+                off += (G[l].nx + 2) * (G[l].ny + 2) * (G[l].nz + 2);
+                T2.boff = off;
+                off += (int)G[l].n;
+                T2.w = tail_w_->as<double>() + woff;
+                woff += 8 * G[l].n;
+            }
             tail_smem_ = (size_t)off * sizeof(double);
             tail_out_.reset(new DevMem(G[Lt].n * sizeof(T)));
             bytes_ += G[Lt].n * sizeof(T);
             if (tail_smem_ > 48 * 1024) {
-                MF3D_CK(cudaFuncSetAttribute(tail_kernel<T, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                MF3D_CK(cudaFuncSetAttribute(tail2_kernel<T, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)tail_smem_));
-                MF3D_CK(cudaFuncSetAttribute(tail_kernel<double, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                MF3D_CK(cudaFuncSetAttribute(tail2_kernel<double, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)tail_smem_));
             }
         }
     }
 
     void build_coefs(cudaStream_t s, const std::vector<const double*>& Klev) override {
-        if (std::is_same<TC, double>::value) return;
-        for (int l = 0; l < Lt_; ++l) launch_faces<TC>(s, G_[l], Klev[l], bc_, scale_[l], ops_[l]);
+        if (!std::is_same<TC, double>::value)
+            for (int l = 0; l < Lt_; ++l) launch_faces<TC>(s, G_[l], Klev[l], bc_, scale_[l], ops_[l]);
+        for (int l = Lt_; l < (int)G_.size(); ++l) {
+            tail_weights_kernel<<<grid1d(G_[l].n, 256), 256, 0, s>>>(op64_[l], (double*)tail_.L[l - Lt_].w);
+            MF3D_LAUNCH_CK();
+        }
     }
 
     size_t z_elt() const override { return sizeof(T); }
     size_t bytes() const override { return bytes_; }
+    int tma_levels() const override { return n_tma_; }
 
-    void run(cudaStream_t s, const double* r, void* zv, double* rho_out) override {
+    void run(cudaStream_t s, void* zv, double* rho_out) override {
         T* z = (T*)zv;
         const int nl = (int)G_.size();
         std::vector<const T*> cur(Lt_ + 1, nullptr), fin(Lt_ + 1, nullptr);
@@ -319,26 +413,21 @@ template <class T, class TC> class VCycle : public VCycleBase {
             T* bc_next = (T*)bl_[l + 1]->p;
             const T* c = nullptr;
             for (int sw = 1; sw <= pre_; ++sw) {
-                T* out = (c == (const T*)xa_[l]->p) ? (T*)xb_[l]->p : (T*)xa_[l]->p;
+                T* out = other(l, c);
                 int mode = (c ? 0 : M_ZERO) | (sw == pre_ ? M_RESID : 0);
-                sweep(s, l, r, c, out, nullptr, bc_next, mode, nullptr);
+                sweep(s, l, c, out, nullptr, bc_next, mode, nullptr);
                 c = out;
             }
-            if (pre_ == 0) restrict_b(s, l, r, bc_next);
+            if (pre_ == 0) restrict_b(s, l, bc_next);
             cur[l] = c;
         }
         // ---- tail (coarsest levels in one CTA, FP64) ----
         const T* e_below = nullptr;
         if (Lt_ < nl) {
             T* out = (Lt_ == 0) ? z : (T*)tail_out_->p;
-            if (Lt_ == 0) {
-                tail_kernel<double, T><<<1, TAIL_NT, tail_smem_, s>>>(tail_, r, out);
-            } else {
-                tail_kernel<T, T><<<1, TAIL_NT, tail_smem_, s>>>(tail_, (const T*)bl_[Lt_]->p, out);
-            }
-            MF3D_LAUNCH_CK();
+            launch_tail(s, out);
             e_below = out;
-            if (Lt_ == 0 && rho_out) dot_rz(s, r, z, G_[0].n, rho_out);
+            if (Lt_ == 0 && rho_out) dot_rz(s, z, G_[0].n, rho_out);
         }
         // ---- up ----
         for (int l = Lt_ - 1; l >= 0; --l) {
@@ -346,29 +435,26 @@ template <class T, class TC> class VCycle : public VCycleBase {
             const T* e = (l + 1 == Lt_) ? e_below : fin[l + 1];
             for (int sw = 1; sw <= post_; ++sw) {
                 const bool last = sw == post_;
-                T* out;
-                if (l == 0 && last) out = z;
-                else out = (c == (const T*)xa_[l]->p) ? (T*)xb_[l]->p : (T*)xa_[l]->p;
+                T* out = (l == 0 && last) ? z : other(l, c);
                 int mode = (c ? 0 : M_ZERO) | (sw == 1 ? M_PROLONG : 0) | ((l == 0 && last && rho_out) ? M_DOT : 0);
-                sweep(s, l, r, c, out, e, nullptr, mode, rho_out);
+                sweep(s, l, c, out, e, nullptr, mode, rho_out);
                 c = out;
             }
             if (post_ == 0) {
-                T* out = (l == 0) ? z : ((c == (const T*)xa_[l]->p) ? (T*)xb_[l]->p : (T*)xa_[l]->p);
+                T* out = (l == 0) ? z : other(l, c);
                 prolong_kernel<T><<<grid1d(G_[l].n, 256), 256, 0, s>>>(G_[l].nx, G_[l].ny, G_[l].nz, c, e, out);
                 MF3D_LAUNCH_CK();
                 c = out;
-                if (l == 0 && rho_out) dot_rz(s, r, z, G_[0].n, rho_out);
+                if (l == 0 && rho_out) dot_rz(s, z, G_[0].n, rho_out);
             }
             fin[l] = c;
         }
     }
 
-    void profile(Timer& tm, int reps, const double* r, void* zv, double* rho_out,
-                 std::vector<mf3d_kernel_timing>& out) override {
+    void profile(Timer& tm, int reps, void* zv, double* rho_out, std::vector<mf3d_kernel_timing>& out) override {
         T* z = (T*)zv;
         const int nl = (int)G_.size();
-        out.push_back(timing("vcycle_total", tm.mean_ms(reps, [&] { run(tm.s, r, zv, rho_out); }), 0.0, 1));
+        out.push_back(timing("vcycle_total", tm.mean_ms(reps, [&] { run(tm.s, zv, rho_out); }), 0.0, 1));
         if (Lt_ >= 1) {
             const double n = (double)G_[0].n, et = sizeof(T), ec = sizeof(TC);
             const double coef = 3.0 * n * ec, nc = n / 8.0;
@@ -377,85 +463,111 @@ template <class T, class TC> class VCycle : public VCycleBase {
             T* bc1 = (T*)bl_[1]->p;
             const T* e1 = (Lt_ == 1) ? (const T*)tail_out_->p : (const T*)xa_[1]->p;
             const int pre_extra = std::max(0, pre_ - 2), post_extra = std::max(0, post_ - 2);
+            const char* tag = tma_[0] ? "tma" : "ldg";
+            char nm[40];
             if (pre_ >= 1) {
-                out.push_back(timing("sweep_l0_zero_in", tm.mean_ms(reps, [&] {
-                    sweep(tm.s, 0, r, nullptr, xa, nullptr, bc1, pre_ == 1 ? (M_ZERO | M_RESID) : M_ZERO, nullptr);
-                }), 8.0 * n + coef + et * n + (pre_ == 1 ? et * nc : 0.0), 1));
+                std::snprintf(nm, sizeof(nm), "sweep_l0_zero_in_%s", tag);
+                out.push_back(timing(nm, tm.mean_ms(reps, [&] {
+                    sweep(tm.s, 0, nullptr, xa, nullptr, bc1, pre_ == 1 ? (M_ZERO | M_RESID) : M_ZERO, nullptr);
+                }), et * n + coef + et * n + (pre_ == 1 ? et * nc : 0.0), 1));
             }
             if (pre_ >= 2) {
-                out.push_back(timing("sweep_l0_resid_restrict", tm.mean_ms(reps, [&] {
-                    sweep(tm.s, 0, r, xa, xb, nullptr, bc1, M_RESID, nullptr);
-                }), et * n + 8.0 * n + coef + et * n + et * nc, 1));
+                std::snprintf(nm, sizeof(nm), "sweep_l0_resid_restrict_%s", tag);
+                out.push_back(timing(nm, tm.mean_ms(reps, [&] {
+                    sweep(tm.s, 0, xa, xb, nullptr, bc1, M_RESID, nullptr);
+                }), et * n + et * n + coef + et * n + et * nc, 1));
             }
             if (pre_extra + post_extra > 0) {
-                out.push_back(timing("sweep_l0_plain", tm.mean_ms(reps, [&] {
-                    sweep(tm.s, 0, r, xa, xb, nullptr, nullptr, 0, nullptr);
-                }), et * n + 8.0 * n + coef + et * n, pre_extra + post_extra));
+                std::snprintf(nm, sizeof(nm), "sweep_l0_plain_%s", tag);
+                out.push_back(timing(nm, tm.mean_ms(reps, [&] {
+                    sweep(tm.s, 0, xa, xb, nullptr, nullptr, 0, nullptr);
+                }), et * n + et * n + coef + et * n, pre_extra + post_extra));
             }
             if (post_ >= 2) {
-                out.push_back(timing("sweep_l0_prolong", tm.mean_ms(reps, [&] {
-                    sweep(tm.s, 0, r, xb, xa, e1, nullptr, M_PROLONG, nullptr);
-                }), et * n + et * nc + 8.0 * n + coef + et * n, 1));
+                std::snprintf(nm, sizeof(nm), "sweep_l0_prolong_%s", tag);
+                out.push_back(timing(nm, tm.mean_ms(reps, [&] {
+                    sweep(tm.s, 0, xb, xa, e1, nullptr, M_PROLONG, nullptr);
+                }), et * n + et * nc + et * n + coef + et * n, 1));
             }
             if (post_ >= 1) {
-                out.push_back(timing("sweep_l0_dot_out", tm.mean_ms(reps, [&] {
-                    sweep(tm.s, 0, r, xa, z, e1, nullptr, post_ == 1 ? (M_PROLONG | M_DOT) : M_DOT, rho_out);
-                }), et * n + 8.0 * n + coef + et * n + (post_ == 1 ? et * nc : 0.0), 1));
+                std::snprintf(nm, sizeof(nm), "sweep_l0_dot_out_%s", tag);
+                out.push_back(timing(nm, tm.mean_ms(reps, [&] {
+                    sweep(tm.s, 0, xa, z, e1, nullptr, post_ == 1 ? (M_PROLONG | M_DOT) : M_DOT, rho_out);
+                }), et * n + et * n + coef + et * n + 8.0 * n + (post_ == 1 ? et * nc : 0.0), 1));
             }
-            // every other sweep level, whole
             for (int l = 1; l < Lt_; ++l) {
-                char nm[40];
-                std::snprintf(nm, sizeof(nm), "sweep_l%d_plain", l);
+                std::snprintf(nm, sizeof(nm), "sweep_l%d_plain_%s", l, tma_[l] ? "tma" : "ldg");
                 T* a = (T*)xa_[l]->p;
                 T* b = (T*)xb_[l]->p;
                 const double nn = (double)G_[l].n;
-                out.push_back(timing(nm, tm.mean_ms(reps, [&] { sweep(tm.s, l, r, a, b, nullptr, nullptr, 0, nullptr); }),
+                out.push_back(timing(nm, tm.mean_ms(reps, [&] { sweep(tm.s, l, a, b, nullptr, nullptr, 0, nullptr); }),
                                      3.0 * et * nn + 3.0 * nn * ec, pre_ + post_));
             }
         }
         if (Lt_ < nl) {
             T* outp = (Lt_ == 0) ? z : (T*)tail_out_->p;
-            out.push_back(timing("coarse_tail", tm.mean_ms(reps, [&] {
-                if (Lt_ == 0)
-                    tail_kernel<double, T><<<1, TAIL_NT, tail_smem_, tm.s>>>(tail_, r, outp);
-                else
-                    tail_kernel<T, T><<<1, TAIL_NT, tail_smem_, tm.s>>>(tail_, (const T*)bl_[Lt_]->p, outp);
-                MF3D_LAUNCH_CK();
-            }), 0.0, 1));
+            out.push_back(timing("coarse_tail", tm.mean_ms(reps, [&] { launch_tail(tm.s, outp); }), 0.0, 1));
         }
     }
 
   private:
-    static int zchunk_for(const Geom& g, int nblk_xy) {
-        const int target = num_sms() * 6;
-        int zc = (int)((long long)g.nz * nblk_xy / std::max(1, target));
-        zc = std::max(8, (zc + 1) & ~1);
+    struct Maps4 {
+        TmaMaps xa, xb; // x read from xa or from xb
+    };
+
+    T* other(int l, const T* c) const { return (c == (const T*)xa_[l]->p) ? (T*)xb_[l]->p : (T*)xa_[l]->p; }
+
+    void launch_tail(cudaStream_t s, T* out) {
+        if (Lt_ == 0)
+            tail2_kernel<double, T><<<1, TAIL2_NT, tail_smem_, s>>>(tail_, r64_, out);
+        else
+            tail2_kernel<T, T><<<1, TAIL2_NT, tail_smem_, s>>>(tail_, (const T*)bl_[Lt_]->p, out);
+        MF3D_LAUNCH_CK();
+    }
+
+    static int zchunk_for(const Geom& g, int nblk_xy, int target_blocks) {
+        // about target_blocks CTAs in total, each marching an even number of planes
+        int nzc = std::max(1, (int)std::min<long long>(g.nz, std::max(1, target_blocks / std::max(1, nblk_xy))));
+        int zc = (g.nz + nzc - 1) / nzc;
+        zc = std::max(2, (zc + 1) & ~1);
         return std::min(zc, ((g.nz + 1) & ~1));
     }
 
-    void sweep(cudaStream_t s, int l, const double* r, const T* x_in, T* x_out, const T* e, T* b_coarse, int mode,
-               double* dot_out) {
+    void sweep(cudaStream_t s, int l, const T* x_in, T* x_out, const T* e, T* b_coarse, int mode, double* dot_out) {
         const Geom& g = G_[l];
         const int gx = (g.nx + SW_TX - 1) / SW_TX, gy = (g.ny + SW_TY - 1) / SW_TY;
-        const int zc = zchunk_for(g, gx * gy);
+        const bool tma = tma_[l] != 0;
+        // the staged sweep keeps two CTAs per SM busy; the load-per-stage sweep wants many
+        const int zc = zchunk_for(g, gx * gy, num_sms() * (tma ? 8 : 6));
         const int gz = (g.nz + zc - 1) / zc;
         dim3 grid(gx, gy, gz);
         const unsigned nblk = (unsigned)gx * gy * gz;
         if ((mode & M_DOT) && nblk > scr_.partial_cap) throw Error(MF3D_E_INVALID, "reduction scratch too small");
-        if (l == 0) {
-            SweepArgs<T, TC, double> a{};
-            fill(a, l, r, x_in, x_out, e, b_coarse, zc, dot_out);
-            dispatch<double>(s, grid, mode, a);
-        } else {
-            SweepArgs<T, TC, T> a{};
-            fill(a, l, (const T*)bl_[l]->p, x_in, x_out, e, b_coarse, zc, dot_out);
-            dispatch<T>(s, grid, mode, a);
+        const T* b = l == 0 ? b0_ : (const T*)bl_[l]->p;
+        if (tma) {
+            TmaSweepArgs<T, TC> a{};
+            a.L = ops_[l];
+            a.x_out = x_out;
+            a.e_c = e;
+            if (l + 1 < (int)G_.size()) {
+                a.ncx = G_[l + 1].nx;
+                a.ncy = G_[l + 1].ny;
+            }
+            a.b_coarse = b_coarse;
+            a.zchunk = zc;
+            a.r64 = r64_;
+            a.dot_partials = scr_.partials;
+            a.dot_ticket = scr_.tickets + 0;
+            a.dot_out = dot_out;
+            a.err = scr_.err;
+            const Maps4& m4 = maps_[l][(mode & M_RESID) ? 1 : 0];
+            const TmaMaps& maps = (x_in == (const T*)xb_[l]->p) ? m4.xb : m4.xa;
+            if (x_in && x_in != (const T*)xa_[l]->p && x_in != (const T*)xb_[l]->p)
+                throw Error(MF3D_E_INVALID, "sweep input is not a level buffer");
+            dispatch_tma(s, grid, mode, maps, a);
+            return;
         }
-    }
-
-    template <class TB>
-    void fill(SweepArgs<T, TC, TB>& a, int l, const TB* b, const T* x_in, T* x_out, const T* e, T* b_coarse, int zc,
-              double* dot_out) {
+        SweepArgs<T, TC, T> a{};
         a.L = ops_[l];
         a.b = b;
         a.x_in = x_in;
@@ -470,37 +582,76 @@ template <class T, class TC> class VCycle : public VCycleBase {
         a.dot_partials = scr_.partials;
         a.dot_ticket = scr_.tickets + 0;
         a.dot_out = dot_out;
+        a.r64 = r64_;
+        dispatch(s, grid, mode, a);
     }
 
-    template <class TB> void dispatch(cudaStream_t s, dim3 grid, int mode, const SweepArgs<T, TC, TB>& a) {
+    template <int MODE> static void set_one() {
+        MF3D_CK(cudaFuncSetAttribute(sweep_tma_kernel<T, TC, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)TmaSweepCfg<T, TC, MODE>::SMEM));
+    }
+    static void set_tma_smem() {
+        set_one<0>();
+        set_one<M_ZERO>();
+        set_one<M_PROLONG>();
+        set_one<M_ZERO | M_PROLONG>();
+        set_one<M_RESID>();
+        set_one<M_ZERO | M_RESID>();
+        set_one<M_DOT>();
+        set_one<M_ZERO | M_DOT>();
+        set_one<M_PROLONG | M_DOT>();
+        set_one<M_ZERO | M_PROLONG | M_DOT>();
+    }
+
+    template <int MODE>
+    static void launch_tma(cudaStream_t s, dim3 grid, const TmaMaps& m, const TmaSweepArgs<T, TC>& a) {
+        sweep_tma_kernel<T, TC, MODE><<<grid, SW_NT, TmaSweepCfg<T, TC, MODE>::SMEM, s>>>(m, a);
+    }
+
+    void dispatch_tma(cudaStream_t s, dim3 grid, int mode, const TmaMaps& m, const TmaSweepArgs<T, TC>& a) {
         switch (mode) {
-        case 0: sweep_kernel<T, TC, TB, 0><<<grid, SW_NT, 0, s>>>(a); break;
-        case M_ZERO: sweep_kernel<T, TC, TB, M_ZERO><<<grid, SW_NT, 0, s>>>(a); break;
-        case M_PROLONG: sweep_kernel<T, TC, TB, M_PROLONG><<<grid, SW_NT, 0, s>>>(a); break;
-        case M_ZERO | M_PROLONG: sweep_kernel<T, TC, TB, M_ZERO | M_PROLONG><<<grid, SW_NT, 0, s>>>(a); break;
-        case M_RESID: sweep_kernel<T, TC, TB, M_RESID><<<grid, SW_NT, 0, s>>>(a); break;
-        case M_ZERO | M_RESID: sweep_kernel<T, TC, TB, M_ZERO | M_RESID><<<grid, SW_NT, 0, s>>>(a); break;
-        case M_DOT: sweep_kernel<T, TC, TB, M_DOT><<<grid, SW_NT, 0, s>>>(a); break;
-        case M_ZERO | M_DOT: sweep_kernel<T, TC, TB, M_ZERO | M_DOT><<<grid, SW_NT, 0, s>>>(a); break;
-        case M_PROLONG | M_DOT: sweep_kernel<T, TC, TB, M_PROLONG | M_DOT><<<grid, SW_NT, 0, s>>>(a); break;
+        case 0: launch_tma<0>(s, grid, m, a); break;
+        case M_ZERO: launch_tma<M_ZERO>(s, grid, m, a); break;
+        case M_PROLONG: launch_tma<M_PROLONG>(s, grid, m, a); break;
+        case M_ZERO | M_PROLONG: launch_tma<M_ZERO | M_PROLONG>(s, grid, m, a); break;
+        case M_RESID: launch_tma<M_RESID>(s, grid, m, a); break;
+        case M_ZERO | M_RESID: launch_tma<M_ZERO | M_RESID>(s, grid, m, a); break;
+        case M_DOT: launch_tma<M_DOT>(s, grid, m, a); break;
+        case M_ZERO | M_DOT: launch_tma<M_ZERO | M_DOT>(s, grid, m, a); break;
+        case M_PROLONG | M_DOT: launch_tma<M_PROLONG | M_DOT>(s, grid, m, a); break;
+        case M_ZERO | M_PROLONG | M_DOT: launch_tma<M_ZERO | M_PROLONG | M_DOT>(s, grid, m, a); break;
+        default: throw Error(MF3D_E_INVALID, "unsupported sweep mode");
+        }
+        MF3D_LAUNCH_CK();
+    }
+
+    void dispatch(cudaStream_t s, dim3 grid, int mode, const SweepArgs<T, TC, T>& a) {
+        switch (mode) {
+        case 0: sweep_kernel<T, TC, T, 0><<<grid, SW_NT, 0, s>>>(a); break;
+        case M_ZERO: sweep_kernel<T, TC, T, M_ZERO><<<grid, SW_NT, 0, s>>>(a); break;
+        case M_PROLONG: sweep_kernel<T, TC, T, M_PROLONG><<<grid, SW_NT, 0, s>>>(a); break;
+        case M_ZERO | M_PROLONG: sweep_kernel<T, TC, T, M_ZERO | M_PROLONG><<<grid, SW_NT, 0, s>>>(a); break;
+        case M_RESID: sweep_kernel<T, TC, T, M_RESID><<<grid, SW_NT, 0, s>>>(a); break;
+        case M_ZERO | M_RESID: sweep_kernel<T, TC, T, M_ZERO | M_RESID><<<grid, SW_NT, 0, s>>>(a); break;
+        case M_DOT: sweep_kernel<T, TC, T, M_DOT><<<grid, SW_NT, 0, s>>>(a); break;
+        case M_ZERO | M_DOT: sweep_kernel<T, TC, T, M_ZERO | M_DOT><<<grid, SW_NT, 0, s>>>(a); break;
+        case M_PROLONG | M_DOT: sweep_kernel<T, TC, T, M_PROLONG | M_DOT><<<grid, SW_NT, 0, s>>>(a); break;
         case M_ZERO | M_PROLONG | M_DOT:
-            sweep_kernel<T, TC, TB, M_ZERO | M_PROLONG | M_DOT><<<grid, SW_NT, 0, s>>>(a);
+            sweep_kernel<T, TC, T, M_ZERO | M_PROLONG | M_DOT><<<grid, SW_NT, 0, s>>>(a);
             break;
         default: throw Error(MF3D_E_INVALID, "unsupported sweep mode");
         }
         MF3D_LAUNCH_CK();
     }
 
-    void restrict_b(cudaStream_t s, int l, const double* r, T* out) {
+    void restrict_b(cudaStream_t s, int l, T* out) {
         const Geom& c = G_[l + 1];
-        if (l == 0)
-            restrict_kernel<T, double><<<grid1d(c.n, 256), 256, 0, s>>>(c.nx, c.ny, c.nz, r, out);
-        else
-            restrict_kernel<T, T><<<grid1d(c.n, 256), 256, 0, s>>>(c.nx, c.ny, c.nz, (const T*)bl_[l]->p, out);
+        const T* fine = l == 0 ? b0_ : (const T*)bl_[l]->p;
+        restrict_kernel<T, T><<<grid1d(c.n, 256), 256, 0, s>>>(c.nx, c.ny, c.nz, fine, out);
         MF3D_LAUNCH_CK();
     }
 
-    void dot_rz(cudaStream_t s, const double* r, const T* z, size_t n, double* out);
+    void dot_rz(cudaStream_t s, const T* z, size_t n, double* out);
 
     std::vector<Geom> G_;
     int Lt_;
@@ -509,12 +660,17 @@ template <class T, class TC> class VCycle : public VCycleBase {
     int pre_, post_, coarse_;
     std::vector<LevelOp<double>> op64_;
     Scratch scr_;
+    const T* b0_;
+    const double* r64_;
     std::vector<LevelOp<TC>> ops_;
     std::vector<double> scale_;
     std::vector<std::unique_ptr<CoefStore>> coef_;
     std::vector<std::unique_ptr<DevMem>> xa_, xb_, bl_;
-    std::unique_ptr<DevMem> tail_out_;
-    TailArgs tail_{};
+    std::vector<int> tma_;
+    std::vector<std::array<Maps4, 2>> maps_;
+    int n_tma_ = 0;
+    std::unique_ptr<DevMem> tail_out_, tail_w_;
+    Tail2Args tail_{};
     size_t tail_smem_ = 0;
     size_t bytes_ = 0;
 };
@@ -530,9 +686,9 @@ __global__ void dot_kernel(size_t n, const double* __restrict__ a, const T* __re
 }
 
 template <class T, class TC>
-void VCycle<T, TC>::dot_rz(cudaStream_t s, const double* r, const T* z, size_t n, double* out) {
+void VCycle<T, TC>::dot_rz(cudaStream_t s, const T* z, size_t n, double* out) {
     const unsigned nb = std::min<unsigned>(grid1d(n, PK_NT), (unsigned)scr_.partial_cap);
-    dot_kernel<T><<<nb, PK_NT, 0, s>>>(n, r, z, scr_.partials, scr_.tickets + 1, out);
+    dot_kernel<T><<<nb, PK_NT, 0, s>>>(n, r64_, z, scr_.partials, scr_.tickets + 1, out);
     MF3D_LAUNCH_CK();
 }
 
@@ -558,15 +714,18 @@ class HeadSolver {
         pin_ = pin_enabled(cfg.pin_mode, bc);
         G_ = make_levels(g, cfg.mg_levels);
         const int nl = (int)G_.size();
-        // coarse tail: the smallest suffix of levels whose x and b fit in shared memory
+        // coarse tail: the levels of at most 4096 cells whose padded x and b fit in shared memory
+        auto tail_bytes = [&](int l) {
+            return (size_t)8 * ((size_t)(G_[l].nx + 2) * (G_[l].ny + 2) * (G_[l].nz + 2) + G_[l].n);
+        };
         Lt_ = nl - 1;
-        size_t cells = G_[nl - 1].n;
-        while (Lt_ > 0 && G_[Lt_ - 1].n <= 4096 && cells + G_[Lt_ - 1].n <= 12288) {
+        size_t tbytes = tail_bytes(nl - 1);
+        while (Lt_ > 0 && G_[Lt_ - 1].n <= 4096 && tbytes + tail_bytes(Lt_ - 1) <= 200 * 1024) {
             --Lt_;
-            cells += G_[Lt_].n;
+            tbytes += tail_bytes(Lt_);
         }
-        if (cells > 12288) throw Error(MF3D_E_INVALID, "coarsest level too large for the coarse solver "
-                                                       "(raise mg_levels)");
+        if (tbytes > 200 * 1024)
+            throw Error(MF3D_E_INVALID, "coarsest level too large for the coarse solver (raise mg_levels)");
         if (user_stream) {
             stream_ = user_stream;
         } else {
@@ -614,17 +773,25 @@ class HeadSolver {
         MF3D_CK(cudaMemsetAsync(tickets_.p, 0, tickets_.bytes, stream_));
         MF3D_CK(cudaMemsetAsync(state_.p, 0, state_.bytes, stream_));
         bytes_ += partials_.bytes;
-        Scratch scr{partials_.as<double>(), tickets_.as<unsigned>() + 8, cap};
+        err_.alloc(sizeof(int) * 4);
+        MF3D_CK(cudaMemsetAsync(err_.p, 0, err_.bytes, stream_));
+        Scratch scr{partials_.as<double>(), tickets_.as<unsigned>() + 8, cap, err_.as<int>()};
         const int prec = cfg.precision;
+        const bool tma = std::getenv("MF3D_NO_TMA") == nullptr;
+        if (prec != MF3D_PREC_FP64) {
+            r32_.alloc(n * sizeof(float));
+            bytes_ += r32_.bytes;
+        }
         if (prec == MF3D_PREC_FP64)
             vc_.reset(new VCycle<double, double>(G_, Lt_, bc, pin_, cfg.mg_pre_smooth, cfg.mg_post_smooth,
-                                                 cfg.mg_coarse_iters, op64_, scr));
+                                                 cfg.mg_coarse_iters, op64_, scr, r_.as<double>(), r_.as<double>(), tma));
         else if (prec == MF3D_PREC_FP32)
             vc_.reset(new VCycle<float, float>(G_, Lt_, bc, pin_, cfg.mg_pre_smooth, cfg.mg_post_smooth,
-                                               cfg.mg_coarse_iters, op64_, scr));
+                                               cfg.mg_coarse_iters, op64_, scr, r32_.as<float>(), r_.as<double>(), tma));
         else if (prec == MF3D_PREC_BF16)
             vc_.reset(new VCycle<float, __nv_bfloat16>(G_, Lt_, bc, pin_, cfg.mg_pre_smooth, cfg.mg_post_smooth,
-                                                       cfg.mg_coarse_iters, op64_, scr));
+                                                       cfg.mg_coarse_iters, op64_, scr, r32_.as<float>(),
+                                                       r_.as<double>(), tma));
         else
             throw Error(MF3D_E_INVALID, "unknown precision");
         bytes_ += vc_->bytes();
@@ -681,14 +848,30 @@ class HeadSolver {
 
     void vcycle(const double* r, double* z) {
         if (!have_K_) throw Error(MF3D_E_STATE, "set_K must be called before vcycle");
+        const size_t n = G_[0].n;
+        MF3D_CK(cudaMemcpyAsync(r_.p, r, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+        if (r32_.p) {
+            convert_kernel<float, double><<<grid1d(n, 256), 256, 0, stream_>>>(n, r_.as<double>(), r32_.as<float>());
+            MF3D_LAUNCH_CK();
+        }
         if (vc_->z_elt() == sizeof(double)) {
-            vc_->run(stream_, r, z, nullptr);
+            vc_->run(stream_, z, nullptr);
         } else {
-            vc_->run(stream_, r, z_.p, nullptr);
-            convert_kernel<double, float><<<grid1d(G_[0].n, 256), 256, 0, stream_>>>(G_[0].n, z_.as<float>(), z);
+            vc_->run(stream_, z_.p, nullptr);
+            convert_kernel<double, float><<<grid1d(n, 256), 256, 0, stream_>>>(n, z_.as<float>(), z);
             MF3D_LAUNCH_CK();
         }
         MF3D_CK(cudaStreamSynchronize(stream_));
+        check_err();
+    }
+
+    void check_err() {
+        int e = 0;
+        MF3D_CK(cudaMemcpy(&e, err_.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e) {
+            MF3D_CK(cudaMemset(err_.p, 0, sizeof(int)));
+            throw Error(MF3D_E_CUDA, "a TMA pipeline wait timed out in the smoother");
+        }
     }
 
     void solve(double* h, const double* x0, mf3d_solve_result* res) {
@@ -724,6 +907,7 @@ class HeadSolver {
         MF3D_CK(cudaEventRecord(ev1_, s));
         MF3D_CK(cudaMemcpyAsync(host_state_, state_.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
         MF3D_CK(cudaStreamSynchronize(s));
+        check_err();
         const PcgState& st = *host_state_;
         long long launches = g_launches - l0;
         if (body_runs < 0) launches += (long long)std::max(st.iter, 1) * body_launches_;
@@ -747,13 +931,16 @@ class HeadSolver {
     // Times each kernel of one PCG iteration on the current state (see mf3d.h).
     std::vector<mf3d_kernel_timing> profile(int reps) {
         if (!have_K_) throw Error(MF3D_E_STATE, "set_K must be called before profile");
+        reps = std::min(reps, std::max(1, cfg_.cg_max_iter - 2)); // stays inside the loop bound
         Timer tm{ev0_, ev1_, stream_};
         std::vector<mf3d_kernel_timing> out;
         const size_t n = G_[0].n;
         PcgState* st = state_.as<PcgState>();
         const double nd = (double)n, ez = (double)vc_->z_elt();
-        vc_->profile(tm, reps, r_.as<double>(), z_.p, &st->rho_new, out);
+        vc_->profile(tm, reps, z_.p, &st->rho_new, out);
         const unsigned nb = grid1d(n, PK_NT);
+        pcg_reopen_kernel<<<1, 1, 0, stream_>>>(st);
+        MF3D_LAUNCH_CK();
         out.push_back(timing("matvec_dot", tm.mean_ms(reps, [&] {
             matvec_dot_kernel<double><<<nb, PK_NT, 0, stream_>>>(op64_[0], p_.as<double>(), Ap_.as<double>(), st,
                                                                  partials_.as<double>(), tickets_.as<unsigned>() + 3);
@@ -772,12 +959,12 @@ class HeadSolver {
                 xr_update_kernel<double><<<nb, PK_NT, 0, stream_>>>(n, x_.as<double>(), p_.as<double>(), r_.as<double>(),
                                                                    Ap_.as<double>(), z_.as<double>(), st,
                                                                    partials_.as<double>(), tickets_.as<unsigned>() + 4,
-                                                                   cond_, 0);
+                                                                   cond_, 0, r32_.as<float>());
             else
                 xr_update_kernel<float><<<nb, PK_NT, 0, stream_>>>(n, x_.as<double>(), p_.as<double>(), r_.as<double>(),
                                                                   Ap_.as<double>(), z_.as<float>(), st,
                                                                   partials_.as<double>(), tickets_.as<unsigned>() + 4,
-                                                                  cond_, 0);
+                                                                  cond_, 0, r32_.as<float>());
             MF3D_LAUNCH_CK();
         }), 48.0 * nd + (flexible_ ? ez * nd : 0.0), 1));
         return out;
@@ -791,7 +978,8 @@ class HeadSolver {
         double* out = mode == 0 ? r_.as<double>() : Ap_.as<double>();
         residual_kernel<double><<<grid1d(n, PK_NT), PK_NT, 0, s>>>(
             op64_[0], x_.as<double>(), b_.as<double>(), out, state_.as<PcgState>(), partials_.as<double>(),
-            tickets_.as<unsigned>() + 2, mode, cfg_.conv_norm == MF3D_CONV_B ? 1 : 0);
+            tickets_.as<unsigned>() + 2, mode, cfg_.conv_norm == MF3D_CONV_B ? 1 : 0,
+            mode == 0 ? r32_.as<float>() : nullptr);
         MF3D_LAUNCH_CK();
     }
 
@@ -799,7 +987,7 @@ class HeadSolver {
     void record_body(cudaStream_t s, bool with_cond) {
         const size_t n = G_[0].n;
         PcgState* st = state_.as<PcgState>();
-        vc_->run(s, r_.as<double>(), z_.p, &st->rho_new);
+        vc_->run(s, z_.p, &st->rho_new);
         const unsigned nb = grid1d(n, PK_NT);
         if (vc_->z_elt() == sizeof(double)) {
             pupdate_kernel<double><<<nb, PK_NT, 0, s>>>(n, z_.as<double>(), p_.as<double>(), st);
@@ -814,12 +1002,12 @@ class HeadSolver {
             xr_update_kernel<double><<<nb, PK_NT, 0, s>>>(n, x_.as<double>(), p_.as<double>(), r_.as<double>(),
                                                           Ap_.as<double>(), z_.as<double>(), st,
                                                           partials_.as<double>(), tickets_.as<unsigned>() + 4,
-                                                          cond_, with_cond ? 1 : 0);
+                                                          cond_, with_cond ? 1 : 0, r32_.as<float>());
         } else {
             xr_update_kernel<float><<<nb, PK_NT, 0, s>>>(n, x_.as<double>(), p_.as<double>(), r_.as<double>(),
                                                          Ap_.as<double>(), z_.as<float>(), st,
                                                          partials_.as<double>(), tickets_.as<unsigned>() + 4,
-                                                         cond_, with_cond ? 1 : 0);
+                                                         cond_, with_cond ? 1 : 0, r32_.as<float>());
         }
         MF3D_LAUNCH_CK();
     }
@@ -868,7 +1056,7 @@ class HeadSolver {
     std::vector<std::unique_ptr<CoefStore>> coef64_;
     std::vector<std::unique_ptr<DevMem>> Klev_;
     DevMem x_, b_, r_, p_, Ap_, x0_, z_;
-    DevMem partials_, tickets_, state_, mb_;
+    DevMem partials_, tickets_, state_, mb_, err_, r32_;
     std::unique_ptr<VCycleBase> vc_;
     PcgState* host_state_ = nullptr;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
