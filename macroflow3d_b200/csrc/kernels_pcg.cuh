@@ -25,6 +25,7 @@ struct PcgState {
     double alpha, beta;
     int iter, max_iter, check_every, flexible;
     int converged, status, stop, body_count;
+    int solver;                    // 0 PCG (preconditioned), 1 plain CG, 2 standalone MG
     unsigned long long t_start_ns; // %globaltimer at the start of the solve
     unsigned long long budget_ns;  // device-time limit of one solve
 };
@@ -39,12 +40,18 @@ __device__ __forceinline__ unsigned long long global_ns() {
 
 constexpr int PK_NT = 256;
 
+__device__ __forceinline__ bool first_thread() {
+    return (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y | threadIdx.z) == 0;
+}
+
 // y = A x with the reference operator (src/numerics/operators/varcoeff_laplacian.cu:38-239):
 // y_c = (sum_f C_f x_f - D_c x_c) / dx^2, and with the pin the diagonal at cell 0 grows by
 // the coefficients of its in-domain faces only (varcoeff_laplacian.cu:225-229).
+// With pin_full the whole diagonal is doubled instead, the smoother's and residual's
+// convention (src/multigrid/smoothers/residual_3d.cu:365-368), used by the standalone MG solver.
 template <class TC>
 __device__ __forceinline__ double apply_A_cell(const LevelOp<TC>& L, const double* __restrict__ x, int i,
-                                               int j, int k, size_t c) {
+                                               int j, int k, size_t c, bool pin_full = false) {
     const size_t nxy = (size_t)L.nx * L.ny;
     double cxm, cxp, cym, cyp, czm, czp;
     cell_coefs<double>(L, i, j, k, c, cxm, cxp, cym, cyp, czm, czp);
@@ -56,8 +63,10 @@ __device__ __forceinline__ double apply_A_cell(const LevelOp<TC>& L, const doubl
     const double xb = k > 0 ? __ldg(x + c - nxy) : (L.per_z ? __ldg(x + c + (size_t)(L.nz - 1) * nxy) : 0.0);
     const double xt = k < L.nz - 1 ? __ldg(x + c + nxy) : (L.per_z ? __ldg(x + c - (size_t)(L.nz - 1) * nxy) : 0.0);
     double D = cxm + cxp + cym + cyp + czm + czp;
-    if (L.pin && c == 0)
-        D += (L.nx > 1 ? cxp : 0.0) + (L.ny > 1 ? cyp : 0.0) + (L.nz > 1 ? czp : 0.0);
+    if (L.pin && c == 0) {
+        if (pin_full) D *= 2.0;
+        else D += (L.nx > 1 ? cxp : 0.0) + (L.ny > 1 ? cyp : 0.0) + (L.nz > 1 ? czp : 0.0);
+    }
     const double s = cxp * xe + cxm * xw + cyp * xn + cym * xs + czp * xt + czm * xb;
     return (s - D * xc) * L.inv_dx2;
 }
@@ -68,20 +77,40 @@ template <class TC>
 __global__ void __launch_bounds__(PK_NT) residual_kernel(const LevelOp<TC> L, const double* __restrict__ x,
                                                          const double* __restrict__ b, double* __restrict__ r,
                                                          PcgState* st, double* partials, unsigned* ticket,
-                                                         int mode, int ref_is_b, float* __restrict__ r32) {
-    const size_t n = (size_t)L.nx * L.ny * L.nz;
+                                                         int mode, int ref_is_b, float* __restrict__ r32,
+                                                         cudaGraphConditionalHandle cond, int use_cond, int zchunk) {
+    const bool mg = st->solver == 2;
+    const bool first = first_thread();
+    if (mode == 2 && st->stop) { // standalone MG: finished before this cycle
+        if (use_cond && first) cudaGraphSetConditional(cond, 0u);
+        return;
+    }
+    if (mode == 2 && first) {
+        // loop bound independent of the reductions (see xr_update_kernel)
+        const int bc = atomicAdd(&st->body_count, 1) + 1;
+        const bool over_time = global_ns() - st->t_start_ns > st->budget_ns;
+        if (bc > st->max_iter + 1 || over_time) {
+            if (over_time) st->status = PCG_TIMEOUT;
+            st->stop = 1;
+            if (use_cond) cudaGraphSetConditional(cond, 0u);
+        }
+    }
     double srr = 0.0, sbb = 0.0;
-    for (size_t c = blockIdx.x * (size_t)PK_NT + threadIdx.x; c < n; c += (size_t)gridDim.x * PK_NT) {
-        const int i = (int)(c % L.nx), j = (int)((c / L.nx) % L.ny), k = (int)(c / ((size_t)L.nx * L.ny));
-        const double bv = b[c];
-        const double rv = bv + (-1.0) * apply_A_cell(L, x, i, j, k, c);
-        r[c] = rv;
-        if (r32) r32[c] = (float)rv;
-        srr += rv * rv;
-        sbb += bv * bv;
+    const Col3 q = col3(L.nx, L.ny, L.nz, zchunk);
+    if (q.ok) {
+        const size_t nxy = (size_t)L.nx * L.ny;
+        for (int k = q.k0; k < q.k1; ++k) {
+            const size_t c = (size_t)q.i + (size_t)L.nx * q.j + nxy * k;
+            const double bv = b[c];
+            const double rv = bv + (-1.0) * apply_A_cell(L, x, q.i, q.j, k, c, mg);
+            r[c] = rv;
+            if (r32) r32[c] = (float)rv;
+            srr += rv * rv;
+            sbb += bv * bv;
+        }
     }
     double v[2] = {srr, sbb}, out[2];
-    if (grid_sums<PK_NT, 2>(v, partials, ticket, gridDim.x, out)) {
+    if (grid_sums<PK_NT, 2>(v, partials, ticket, gridDim.x * gridDim.y * gridDim.z, out)) {
         if (mode == 0) {
             st->r0sq = out[0];
             st->rr = out[0];
@@ -93,11 +122,38 @@ __global__ void __launch_bounds__(PK_NT) residual_kernel(const LevelOp<TC> L, co
             st->status = PCG_OK;
             st->rho_new = st->rho_old = st->gamma = st->pAp = 0.0;
             st->alpha = st->beta = 0.0;
-            // the reference returns at once when ||r0|| < 1e-15 (pcg.cuh:122-127)
-            st->stop = (sqrt(out[0]) < 1e-15 || st->max_iter <= 0) ? 1 : 0;
-            if (sqrt(out[0]) < 1e-15) st->converged = 1;
+            if (st->solver == 2) {
+                // mg_solve has no early exit (src/multigrid/cycle/v_cycle.cu:90-113)
+                st->stop = st->max_iter <= 0 ? 1 : 0;
+            } else {
+                // the reference returns at once when ||r0|| is (near) zero (pcg.cuh:122-127, cg.cuh:61-66)
+                const double r0 = sqrt(out[0]);
+                const bool done = st->solver == 1 ? r0 <= st->rtol * r0 : r0 < 1e-15;
+                st->stop = (done || st->max_iter <= 0) ? 1 : 0;
+                if (done) st->converged = 1;
+                st->rho_new = st->solver == 1 ? out[0] : 0.0; // plain CG: rho = <r, r>
+            }
             if (!isfinite(out[0])) { st->status = PCG_NONFINITE; st->stop = 1; }
             st->t_start_ns = global_ns();
+        } else if (mode == 2) {
+            // one standalone-MG cycle done: x updated, r = b - A x recomputed (v_cycle.cu:100-112)
+            const int it = st->iter + 1;
+            st->iter = it;
+            st->rr = out[0];
+            const double rn = sqrt(out[0]);
+            st->final_res = rn;
+            int stop = 0;
+            if (rn / st->ref_norm < st->rtol) {
+                st->converged = 1;
+                stop = 1;
+            }
+            if (!isfinite(out[0])) {
+                st->status = PCG_NONFINITE;
+                stop = 1;
+            }
+            if (it >= st->max_iter) stop = 1;
+            st->stop = stop;
+            if (use_cond) cudaGraphSetConditional(cond, stop ? 0u : 1u);
         } else {
             st->rr_true = out[0];
         }
@@ -121,18 +177,21 @@ __global__ void __launch_bounds__(PK_NT) pupdate_kernel(size_t n, const TZ* __re
 template <class TC>
 __global__ void __launch_bounds__(PK_NT) matvec_dot_kernel(const LevelOp<TC> L, const double* __restrict__ p,
                                                            double* __restrict__ Ap, PcgState* st,
-                                                           double* partials, unsigned* ticket) {
-    const size_t n = (size_t)L.nx * L.ny * L.nz;
+                                                           double* partials, unsigned* ticket, int zchunk) {
     if (st->stop) return;
     double acc = 0.0;
-    for (size_t c = blockIdx.x * (size_t)PK_NT + threadIdx.x; c < n; c += (size_t)gridDim.x * PK_NT) {
-        const int i = (int)(c % L.nx), j = (int)((c / L.nx) % L.ny), k = (int)(c / ((size_t)L.nx * L.ny));
-        const double y = apply_A_cell(L, p, i, j, k, c);
-        Ap[c] = y;
-        acc += __ldg(p + c) * y;
+    const Col3 q = col3(L.nx, L.ny, L.nz, zchunk);
+    if (q.ok) {
+        const size_t nxy = (size_t)L.nx * L.ny;
+        for (int k = q.k0; k < q.k1; ++k) {
+            const size_t c = (size_t)q.i + (size_t)L.nx * q.j + nxy * k;
+            const double y = apply_A_cell(L, p, q.i, q.j, k, c);
+            Ap[c] = y;
+            acc += __ldg(p + c) * y;
+        }
     }
     double v[1] = {acc}, out[1];
-    if (grid_sums<PK_NT, 1>(v, partials, ticket, gridDim.x, out)) st->pAp = out[0];
+    if (grid_sums<PK_NT, 1>(v, partials, ticket, gridDim.x * gridDim.y * gridDim.z, out)) st->pAp = out[0];
 }
 
 // x += alpha p; r -= alpha Ap (alpha = rho_new / pAp); ||r||^2 and, for the flexible form,
@@ -179,6 +238,7 @@ __global__ void __launch_bounds__(PK_NT) xr_update_kernel(size_t n, double* __re
         st->rr = out[0];
         st->gamma = out[1];
         st->rho_old = s.rho_new;
+        if (s.solver == 1) st->rho_new = out[0]; // plain CG: rho = <r, r> for the next beta
         int stop = 0;
         if (!isfinite(out[0]) || !isfinite(s.pAp) || !isfinite(alpha)) {
             st->status = PCG_NONFINITE;
@@ -190,7 +250,8 @@ __global__ void __launch_bounds__(PK_NT) xr_update_kernel(size_t n, double* __re
         if ((it % s.check_every) == 0 || it >= s.max_iter) {
             const double rn = sqrt(out[0]);
             st->final_res = rn;
-            if (rn / s.ref_norm < s.rtol) {
+            // pcg.cuh:158-160 tests ||r||/||r0|| < rtol; cg.cuh:142-150 tests ||r|| <= rtol ||r0||
+            if (s.solver == 1 ? rn <= s.rtol * s.ref_norm : rn / s.ref_norm < s.rtol) {
                 st->converged = 1;
                 stop = 1;
             }
@@ -206,6 +267,15 @@ __global__ void loop_gate_kernel(const PcgState* st, cudaGraphConditionalHandle 
     cudaGraphSetConditional(cond, st->stop ? 0u : 1u);
 }
 
+// Standalone MG: x += z (the V-cycle of the current residual) unless the loop has stopped.
+template <class TZ>
+__global__ void __launch_bounds__(PK_NT) mg_xupdate_kernel(size_t n, double* __restrict__ x, const TZ* __restrict__ z,
+                                                           const PcgState* st) {
+    if (st->stop) return;
+    for (size_t c = blockIdx.x * (size_t)PK_NT + threadIdx.x; c < n; c += (size_t)gridDim.x * PK_NT)
+        x[c] = x[c] + (double)z[c];
+}
+
 // Re-opens a finished state so the iteration kernels can be timed in isolation (diagnostics).
 __global__ void pcg_reopen_kernel(PcgState* st) {
     st->stop = 0;
@@ -217,7 +287,8 @@ __global__ void pcg_reopen_kernel(PcgState* st) {
 
 // PCG state initialisation (host-given controls).
 __global__ void pcg_init_kernel(PcgState* st, int max_iter, int check_every, int flexible, double rtol,
-                                unsigned long long budget_ns) {
+                                unsigned long long budget_ns, int solver) {
+    st->solver = solver;
     st->max_iter = max_iter;
     st->body_count = 0;
     st->budget_ns = budget_ns;

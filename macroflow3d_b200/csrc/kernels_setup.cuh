@@ -26,11 +26,13 @@ template <> __device__ __forceinline__ __nv_bfloat16 store_coef<__nv_bfloat16>(d
 template <class TC>
 __global__ void faces_kernel(int nx, int ny, int nz, const double* __restrict__ K, BcDev bc, double scale,
                              TC* __restrict__ cx, TC* __restrict__ cy, TC* __restrict__ cz,
-                             TC* __restrict__ bxm, TC* __restrict__ bym, TC* __restrict__ bzm) {
-    const size_t n = (size_t)nx * ny * nz;
+                             TC* __restrict__ bxm, TC* __restrict__ bym, TC* __restrict__ bzm, int zchunk) {
     const size_t nxy = (size_t)nx * ny;
-    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / nxy);
+    const Col3 q = col3(nx, ny, nz, zchunk);
+    if (!q.ok) return;
+    const int i = q.i, j = q.j;
+    for (int k = q.k0; k < q.k1; ++k) {
+        const size_t c = (size_t)i + (size_t)nx * j + nxy * k;
         const double Kc = K[c];
         double v;
         // +x face
@@ -54,12 +56,15 @@ __global__ void faces_kernel(int nx, int ny, int nz, const double* __restrict__ 
 }
 
 // Geometric mean of the 8 children, src/physics/flow/coarsen_K.cu:15-53 (same order).
-__global__ void coarsen_kernel(int NX, int NY, int NZ, const double* __restrict__ Kf, double* __restrict__ Kc) {
-    const size_t n = (size_t)NX * NY * NZ;
+__global__ void coarsen_kernel(int NX, int NY, int NZ, const double* __restrict__ Kf, double* __restrict__ Kc,
+                               int zchunk) {
     const int Nx = 2 * NX;
     const size_t stride = (size_t)Nx * 2 * NY;
-    for (size_t C = blockIdx.x * (size_t)blockDim.x + threadIdx.x; C < n; C += (size_t)gridDim.x * blockDim.x) {
-        const int I = (int)(C % NX), J = (int)((C / NX) % NY), Kk = (int)(C / ((size_t)NX * NY));
+    const Col3 q = col3(NX, NY, NZ, zchunk);
+    if (!q.ok) return;
+    const int I = q.i, J = q.j;
+    for (int Kk = q.k0; Kk < q.k1; ++Kk) {
+        const size_t C = (size_t)I + (size_t)NX * J + (size_t)NX * NY * Kk;
         const size_t i000 = (size_t)(2 * I) + (size_t)Nx * (2 * J) + stride * (2 * Kk);
         const size_t i001 = i000 + stride;
         const double ls = log(Kf[i000]) + log(Kf[i000 + 1]) + log(Kf[i000 + Nx]) + log(Kf[i000 + 1 + Nx]) +
@@ -72,12 +77,14 @@ __global__ void coarsen_kernel(int NX, int NY, int NZ, const double* __restrict_
 // in the order xmin..zmax); x0: the x-linear guess when both x faces are Dirichlet, else 0
 // (src/physics/flow/solve_head.cu:29-73).  x0 may be null.
 __global__ void rhs_guess_kernel(int nx, int ny, int nz, double dx, const double* __restrict__ K, BcDev bc,
-                                 double* __restrict__ b, double* __restrict__ x0) {
-    const size_t n = (size_t)nx * ny * nz;
+                                 double* __restrict__ b, double* __restrict__ x0, int zchunk) {
     const double inv_dx2 = 1.0 / (dx * dx);
     const bool lin = bc.type[0] == BC_DIRICHLET && bc.type[1] == BC_DIRICHLET;
-    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((size_t)nx * ny));
+    const Col3 q = col3(nx, ny, nz, zchunk);
+    if (!q.ok) return;
+    const int i = q.i, j = q.j;
+    for (int k = q.k0; k < q.k1; ++k) {
+        const size_t c = (size_t)i + (size_t)nx * j + (size_t)nx * ny * k;
         const double Kc = K[c];
         double v = 0.0;
         const bool on[6] = {i == 0, i == nx - 1, j == 0, j == ny - 1, k == 0, k == nz - 1};

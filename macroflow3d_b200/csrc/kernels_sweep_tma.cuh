@@ -184,42 +184,70 @@ __global__ void __launch_bounds__(SW_NT) sweep_tma_kernel(const __grid_constant_
     const size_t ncxy = (size_t)a.ncx * a.ncy;
 
     double dot_acc = 0.0;
-    unsigned phase = 0u; // bit s: parity of the next wait on slot s
+    unsigned phase = 0u; // bit s: parity of the next wait on slot s (tracked by thread 0)
 
-    // relaxation of cell (iu, ju, pl) at plane-local element e; sl/slm/slp: slots of pl, pl-1, pl+1
-    auto relax = [&](int iu, int ju, int pl, int e, int sl, int slm, int slp) {
-        const T* x = X(sl);
-        const TC* cx = CX(sl);
-        const TC* cy = CY(sl);
+    // slot base pointers of planes t, t-1, ..., t-4 for the current step
+    unsigned char* pb[5];
+    auto set_bases = [&](int sl_t) {
+#pragma unroll
+        for (int d = 0; d < 5; ++d) {
+            int v = sl_t - d;
+            if (v < 0) v += NR;
+            pb[d] = ring + C::SLOT * v;
+        }
+    };
+    auto Xp = [&](int d) { return (T*)pb[d]; };
+    auto Bp = [&](int d) { return (T*)(pb[d] + C::OB); };
+    auto CXp = [&](int d) { return (TC*)(pb[d] + 2 * C::OB); };
+    auto CYp = [&](int d) { return (TC*)(pb[d] + 2 * C::OB + C::OC); };
+    auto CZp = [&](int d) { return (TC*)(pb[d] + 2 * C::OB + 2 * C::OC); };
+    auto divide = [](T num, T den) -> T {
+        if constexpr (sizeof(T) == 4) return __fdividef(num, den); // preconditioner: 2-ulp division
+        else return num / den;
+    };
+
+    // relaxation of cell (iu, ju, pl) at plane-local element e; d: age of plane pl in the ring
+    auto relax = [&](int iu, int ju, int pl, int e, int d) {
+        T* x = Xp(d);
+        const TC* cx = CXp(d);
+        const TC* cy = CYp(d);
         const T cxp = ld_as_float_or_double<T>(cx[e]);
         const T cyp = ld_as_float_or_double<T>(cy[e]);
-        const T czp = ld_as_float_or_double<T>(CZ(sl)[e]);
+        const T czp = ld_as_float_or_double<T>(CZp(d)[e]);
         const T cxm = iu > 0 ? ld_as_float_or_double<T>(cx[e - 1]) : load_as<T>(L.bxm, (size_t)ju + (size_t)ny * pl);
         const T cym = ju > 0 ? ld_as_float_or_double<T>(cy[e - BX]) : load_as<T>(L.bym, (size_t)iu + (size_t)nx * pl);
-        const T czm = pl > 0 ? ld_as_float_or_double<T>(CZ(slm)[e]) : load_as<T>(L.bzm, (size_t)iu + (size_t)nx * ju);
+        const T czm = pl > 0 ? ld_as_float_or_double<T>(CZp(d + 1)[e]) : load_as<T>(L.bzm, (size_t)iu + (size_t)nx * ju);
         T D = cxm + cxp + cym + cyp + czm + czp;
         if (L.pin && (iu | ju | pl) == 0) D *= (T)2;
-        const T s = cxp * x[e + 1] + cxm * x[e - 1] + cyp * x[e + BX] + cym * x[e - BX] + czp * X(slp)[e] +
-                    czm * X(slm)[e];
-        X(sl)[e] = (s - B(sl)[e] * dx2) / D;
-    };
-    auto back = [&](int s, int d) { // slot d planes before slot s
-        const int v = s - d;
-        return v < 0 ? v + NR : v;
+        const T s = cxp * x[e + 1] + cxm * x[e - 1] + cyp * x[e + BX] + cym * x[e - BX] + czp * Xp(d - 1)[e] +
+                    czm * Xp(d + 1)[e];
+        x[e] = divide(s - Bp(d)[e] * dx2, D);
     };
 
     int sl_t = 0; // slot of plane t
     for (int t = zlo; t <= zhi; ++t) {
-        // ---- wait for plane t ----
-        const bool ok = mbar_wait(&bars[sl_t], (phase >> sl_t) & 1u);
-        phase ^= 1u << sl_t;
+        // ---- thread 0 waits for plane t, refills the ring; the others sleep at the barrier ----
+        bool ok = true;
+        if (tid == 0) {
+            // refill first: plane t-1+PF reuses the slot of plane t-NS-3, which no thread reads
+            // in step t-1 (its oldest plane is t-NS-2) and whose last generic-proxy writes were
+            // fenced before the barriers of step t-1
+            if (t > zlo && t - 1 + PF <= zhi) {
+                int s2 = sl_t - 1 + PF;
+                if (s2 >= NR) s2 -= NR;
+                issue(t - 1 + PF, s2);
+            }
+            ok = mbar_wait(&bars[sl_t], (phase >> sl_t) & 1u);
+            phase ^= 1u << sl_t;
+        }
         if (__syncthreads_or(!ok)) {
             if (tid == 0) atomicExch(a.err, 1);
             return;
         }
+        set_bases(sl_t);
         // ---- zero input / prolongation on the freshly landed x plane ----
         if (ZERO || PROL) {
-            T* x = X(sl_t);
+            T* x = Xp(0);
             const bool in_z = t >= 0 && t < nz;
             const size_t cz_off = ncxy * (size_t)(t >> 1);
 #pragma unroll
@@ -240,25 +268,21 @@ __global__ void __launch_bounds__(SW_NT) sweep_tma_kernel(const __grid_constant_
             if (r_ok && p >= z0 - hr && p <= z1 - 1 + hr && p >= 0 && p < nz) {
                 const int off = (r_par + p) & 1;
                 const int iu = r_iu0 + off;
-                if (iu >= 0 && iu < nx) {
-                    const int sl = back(sl_t, 1);
-                    relax(iu, r_ju, p, r_e0 + off, sl, back(sl, 1), sl_t);
-                }
+                if (iu >= 0 && iu < nx) relax(iu, r_ju, p, r_e0 + off, 1);
             }
         }
         __syncthreads();
         // ---- black at plane q = t-2 (tile + hb), then write the finished plane ----
         const int q = t - 2;
-        const int sl_q = back(sl_t, 2);
         if (b_ok && q >= z0 - hb && q <= z1 - 1 + hb && q >= 0 && q < nz) {
             const int off = ((b_par + q) & 1) ^ 1;
             const int iu = b_iu0 + off;
-            if (iu >= 0 && iu < nx) relax(iu, b_ju, q, b_e0 + off, sl_q, back(sl_q, 1), back(sl_t, 1));
+            if (iu >= 0 && iu < nx) relax(iu, b_ju, q, b_e0 + off, 2);
         }
         __syncthreads();
         if (q >= z0 && q < z1 && o_ok) {
             const size_t c = o_c0 + nxy * q;
-            const T v = X(sl_q)[o_e];
+            const T v = Xp(2)[o_e];
             a.x_out[c] = v;
             if (DOT) dot_acc += __ldg(a.r64 + c) * (double)v;
         }
@@ -266,24 +290,23 @@ __global__ void __launch_bounds__(SW_NT) sweep_tma_kernel(const __grid_constant_
         if (RESID) {
             const int s = t - 3;
             if (s >= z0 && s < z1) {
-                const int sl = back(sl_t, 3), slm = back(sl_t, 4), slp = back(sl_t, 2);
                 T rv = (T)0;
                 if (o_ok) {
                     const int e = o_e;
-                    const T* x = X(sl);
-                    const TC* cx = CX(sl);
-                    const TC* cy = CY(sl);
+                    const T* x = Xp(3);
+                    const TC* cx = CXp(3);
+                    const TC* cy = CYp(3);
                     const T cxp = ld_as_float_or_double<T>(cx[e]);
                     const T cyp = ld_as_float_or_double<T>(cy[e]);
-                    const T czp = ld_as_float_or_double<T>(CZ(sl)[e]);
+                    const T czp = ld_as_float_or_double<T>(CZp(3)[e]);
                     const T cxm = o_gi > 0 ? ld_as_float_or_double<T>(cx[e - 1]) : load_as<T>(L.bxm, (size_t)o_gj + (size_t)ny * s);
                     const T cym = o_gj > 0 ? ld_as_float_or_double<T>(cy[e - BX]) : load_as<T>(L.bym, (size_t)o_gi + (size_t)nx * s);
-                    const T czm = s > 0 ? ld_as_float_or_double<T>(CZ(slm)[e]) : load_as<T>(L.bzm, o_c0);
+                    const T czm = s > 0 ? ld_as_float_or_double<T>(CZp(4)[e]) : load_as<T>(L.bzm, o_c0);
                     T D = cxm + cxp + cym + cyp + czm + czp;
                     if (L.pin && (o_gi | o_gj | s) == 0) D *= (T)2;
                     const T sum = cxp * x[e + 1] + cxm * x[e - 1] + cyp * x[e + BX] + cym * x[e - BX] +
-                                  czp * X(slp)[e] + czm * X(slm)[e];
-                    rv = B(sl)[e] - (sum - D * x[e]) * (T)L.inv_dx2;
+                                  czp * Xp(2)[e] + czm * Xp(4)[e];
+                    rv = Bp(3)[e] - (sum - D * x[e]) * (T)L.inv_dx2;
                 }
                 rsb[((s - z0) & 1) * SW_TX * SW_TY + tid] = rv;
                 if (((s - z0) & 1) == 1) {
@@ -311,14 +334,10 @@ __global__ void __launch_bounds__(SW_NT) sweep_tma_kernel(const __grid_constant_
                 }
             }
         }
-        // generic-proxy writes to the ring (relaxations, fix-ups) are ordered before the TMA
-        // writes that will reuse the slot
+        // generic-proxy writes to the ring are ordered before the TMA writes that reuse the
+        // slot; the barrier at the top of the next step completes the hand-off
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        // ---- refill: the slot of plane t - NS - 1 is dead now ----
-        const int sl_next = (sl_t + 1 == NR) ? 0 : sl_t + 1;
-        if (tid == 0 && t + PF <= zhi) issue(t + PF, (sl_t + PF) % NR);
-        sl_t = sl_next;
+        sl_t = (sl_t + 1 == NR) ? 0 : sl_t + 1;
     }
 
     if (DOT) {

@@ -57,13 +57,15 @@ constexpr int VEL_NT = 256;
 __global__ void __launch_bounds__(VEL_NT) velocity_kernel(int nx, int ny, int nz, double dx,
                                                           const double* __restrict__ H, const double* __restrict__ K,
                                                           BcDev bc, VelOut o, unsigned long long* mb_max,
-                                                          double* partials, unsigned* ticket, double* mb_sums) {
-    const size_t n = (size_t)nx * ny * nz;
+                                                          double* partials, unsigned* ticket, double* mb_sums,
+                                                          int zchunk) {
     const size_t nxy = (size_t)nx * ny;
     double qin = 0.0, qout = 0.0, mx = 0.0;
     const double A = dx * dx;
-    for (size_t c = blockIdx.x * (size_t)VEL_NT + threadIdx.x; c < n; c += (size_t)gridDim.x * VEL_NT) {
-        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / nxy);
+    const Col3 q = col3(nx, ny, nz, zchunk);
+    const int i = q.i, j = q.j;
+    for (int k = q.k0; q.ok && k < q.k1; ++k) {
+        const size_t c = (size_t)i + (size_t)nx * j + nxy * k;
         const double u0 = face_min(H, K, c, c - 1, c + (nx - 1), i == 0, bc.type[0], bc.value[0], dx);
         const double v0 = face_min(H, K, c, c - nx, c + (size_t)(ny - 1) * nx, j == 0, bc.type[2], bc.value[2], dx);
         const double w0 = face_min(H, K, c, c - nxy, c + (size_t)(nz - 1) * nxy, k == 0, bc.type[4], bc.value[4], dx);
@@ -98,8 +100,8 @@ __global__ void __launch_bounds__(VEL_NT) velocity_kernel(int nx, int ny, int nz
         double v[2] = {qin, qout}, out[2];
         // max: non-negative doubles order like their bit patterns
         for (int ofs = 16; ofs > 0; ofs >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, ofs));
-        if ((threadIdx.x & 31) == 0) atomicMax(mb_max, (unsigned long long)__double_as_longlong(mx));
-        if (grid_sums<VEL_NT, 2>(v, partials, ticket, gridDim.x, out)) {
+        if (threadIdx.x == 0) atomicMax(mb_max, (unsigned long long)__double_as_longlong(mx)); // lane 0 of each warp row
+        if (grid_sums<VEL_NT, 2>(v, partials, ticket, gridDim.x * gridDim.y * gridDim.z, out)) {
             mb_sums[0] = out[0];
             mb_sums[1] = out[1];
         }

@@ -103,12 +103,13 @@ __device__ __forceinline__ void cell_coefs(const LevelOp<TC>& L, int i, int j, i
 // ---------------------------------------------------------------------------------------
 template <int NT>
 __device__ __forceinline__ double block_sum(double v, double* red /* NT/32 doubles */) {
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const int w = tid >> 5, l = tid & 31;
     if (l == 0) red[w] = v;
     __syncthreads();
     double s = 0.0;
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
         for (int i = 0; i < NT / 32; ++i) s += red[i];
     }
     __syncthreads();
@@ -116,17 +117,19 @@ __device__ __forceinline__ double block_sum(double v, double* red /* NT/32 doubl
 }
 
 // Returns true on thread 0 of the last block to finish; `out` then holds the grid sums.
+// Blocks may be 1-, 2- or 3-D; NT is the number of threads per block.
 template <int NT, int NV>
 __device__ __forceinline__ bool grid_sums(const double (&v)[NV], double* partials, unsigned* ticket,
                                           int nblocks, double (&out)[NV]) {
     __shared__ double red[NT / 32];
     __shared__ bool s_last;
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
     const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     for (int q = 0; q < NV; ++q) {
         double s = block_sum<NT>(v[q], red);
-        if (threadIdx.x == 0) partials[(size_t)q * nblocks + bid] = s;
+        if (tid == 0) partials[(size_t)q * nblocks + bid] = s;
     }
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
         __threadfence();
         unsigned t = atomicAdd(ticket, 1u);
         s_last = (t == (unsigned)nblocks - 1);
@@ -136,11 +139,27 @@ __device__ __forceinline__ bool grid_sums(const double (&v)[NV], double* partial
     __threadfence();
     for (int q = 0; q < NV; ++q) {
         double acc = 0.0;
-        for (int b = threadIdx.x; b < nblocks; b += NT) acc += __ldcg(partials + (size_t)q * nblocks + b);
+        for (int b = tid; b < nblocks; b += NT) acc += __ldcg(partials + (size_t)q * nblocks + b);
         out[q] = block_sum<NT>(acc, red);
     }
-    if (threadIdx.x == 0) *ticket = 0u;
-    return threadIdx.x == 0;
+    if (tid == 0) *ticket = 0u;
+    return tid == 0;
+}
+
+// 3-D launch shape used by the cell kernels: 32 x 8 threads per (x, y) tile, each thread
+// marching `zchunk` planes of its column (no integer division per cell).
+struct Col3 {
+    int i, j, k0, k1;
+    bool ok;
+};
+__device__ __forceinline__ Col3 col3(int nx, int ny, int nz, int zchunk) {
+    Col3 c;
+    c.i = blockIdx.x * 32 + threadIdx.x;
+    c.j = blockIdx.y * 8 + threadIdx.y;
+    c.k0 = blockIdx.z * zchunk;
+    c.k1 = min(c.k0 + zchunk, nz);
+    c.ok = c.i < nx && c.j < ny;
+    return c;
 }
 
 } // namespace mf3d

@@ -73,6 +73,25 @@ static unsigned grid1d(size_t n, int nt, int per_sm = 8) {
     return (unsigned)std::max<size_t>(1, std::min(want, cap));
 }
 
+// 3-D launch of the column-marching cell kernels: 32 x 8 threads per (x, y) tile, about
+// per_sm * SMs blocks in total, each thread marching zchunk planes.
+struct ColLaunch {
+    dim3 grid, block;
+    int zchunk;
+    unsigned nblocks;
+};
+static ColLaunch col_launch(int nx, int ny, int nz, int per_sm = 8) {
+    ColLaunch L;
+    const long long gx = (nx + 31) / 32, gy = (ny + 7) / 8, bxy = gx * gy;
+    long long nzc = std::max<long long>(1, std::min<long long>(nz, (long long)num_sms() * per_sm / std::max(1LL, bxy)));
+    L.zchunk = (int)((nz + nzc - 1) / nzc);
+    nzc = (nz + L.zchunk - 1) / L.zchunk;
+    L.grid = dim3((unsigned)gx, (unsigned)gy, (unsigned)nzc);
+    L.block = dim3(32, 8, 1);
+    L.nblocks = (unsigned)(bxy * nzc);
+    return L;
+}
+
 // RAII device allocation
 struct DevMem {
     void* p = nullptr;
@@ -187,8 +206,9 @@ struct CoefStore {
 template <class TC>
 static void launch_faces(cudaStream_t s, const Geom& G, const double* K, const mf3d_bc& bc, double scale,
                          const LevelOp<TC>& L) {
-    faces_kernel<TC><<<grid1d(G.n, 256), 256, 0, s>>>(G.nx, G.ny, G.nz, K, to_dev(bc), scale, (TC*)L.cx,
-                                                       (TC*)L.cy, (TC*)L.cz, (TC*)L.bxm, (TC*)L.bym, (TC*)L.bzm);
+    const ColLaunch cl = col_launch(G.nx, G.ny, G.nz);
+    faces_kernel<TC><<<cl.grid, cl.block, 0, s>>>(G.nx, G.ny, G.nz, K, to_dev(bc), scale, (TC*)L.cx, (TC*)L.cy,
+                                                  (TC*)L.cz, (TC*)L.bxm, (TC*)L.bym, (TC*)L.bzm, cl.zchunk);
     MF3D_LAUNCH_CK();
 }
 
@@ -702,8 +722,8 @@ class HeadSolver {
         if (g.nx < 2 || g.ny < 2 || g.nz < 2) throw Error(MF3D_E_INVALID, "grid must have at least 2 cells per axis");
         if (!(g.dx > 0)) throw Error(MF3D_E_INVALID, "dx must be positive");
         validate_bc(bc);
-        if (cfg.solver != MF3D_SOLVER_PCG_MG)
-            throw Error(MF3D_E_INVALID, "only the PCG_MG solver is implemented on this path");
+        if (cfg.solver != MF3D_SOLVER_PCG_MG && cfg.solver != MF3D_SOLVER_MG && cfg.solver != MF3D_SOLVER_CG)
+            throw Error(MF3D_E_INVALID, "unknown solver type");
         if (cfg.mg_pre_smooth < 0 || cfg.mg_post_smooth < 0 || cfg.mg_coarse_iters < 0 || cfg.cg_max_iter < 0)
             throw Error(MF3D_E_INVALID, "negative iteration count");
         for (int a = 0; a < 3; ++a) {
@@ -761,7 +781,7 @@ class HeadSolver {
         vec(Ap_);
         vec(x0_);
         // reduction scratch sized for the largest grid any reduction uses
-        size_t cap = (size_t)grid1d(n, PK_NT) * 2 + 1024;
+        size_t cap = std::max<size_t>((size_t)grid1d(n, PK_NT) * 2, col_launch(G_[0].nx, G_[0].ny, G_[0].nz).nblocks) + 1024;
         {
             const int gx = (G_[0].nx + SW_TX - 1) / SW_TX, gy = (G_[0].ny + SW_TY - 1) / SW_TY;
             cap = std::max(cap, (size_t)gx * gy * (size_t)((G_[0].nz + 7) / 8) + 1024);
@@ -828,8 +848,9 @@ class HeadSolver {
         MF3D_CK(cudaMemcpyAsync(Klev_[0]->p, K, G_[0].n * sizeof(double), cudaMemcpyDeviceToDevice, s));
         for (int l = 0; l + 1 < nl; ++l) {
             const Geom& c = G_[l + 1];
-            coarsen_kernel<<<grid1d(c.n, 256), 256, 0, s>>>(c.nx, c.ny, c.nz, Klev_[l]->as<double>(),
-                                                            Klev_[l + 1]->as<double>());
+            const ColLaunch cl = col_launch(c.nx, c.ny, c.nz);
+            coarsen_kernel<<<cl.grid, cl.block, 0, s>>>(c.nx, c.ny, c.nz, Klev_[l]->as<double>(),
+                                                        Klev_[l + 1]->as<double>(), cl.zchunk);
             MF3D_LAUNCH_CK();
         }
         std::vector<const double*> Kp(nl);
@@ -837,8 +858,11 @@ class HeadSolver {
         for (int l = 0; l < nl; ++l)
             if (coef64_[l]) launch_faces<double>(s, G_[l], Kp[l], bc_, 1.0, op64_[l]);
         vc_->build_coefs(s, Kp);
-        rhs_guess_kernel<<<grid1d(G_[0].n, 256), 256, 0, s>>>(G_[0].nx, G_[0].ny, G_[0].nz, G_[0].dx, Kp[0],
-                                                              to_dev(bc_), b_.as<double>(), x0_.as<double>());
+        {
+            const ColLaunch cl = col_launch(G_[0].nx, G_[0].ny, G_[0].nz);
+            rhs_guess_kernel<<<cl.grid, cl.block, 0, s>>>(G_[0].nx, G_[0].ny, G_[0].nz, G_[0].dx, Kp[0], to_dev(bc_),
+                                                          b_.as<double>(), x0_.as<double>(), cl.zchunk);
+        }
         MF3D_LAUNCH_CK();
         setup_launches_ = (int)(g_launches - l0);
         have_K_ = true;
@@ -884,8 +908,10 @@ class HeadSolver {
         MF3D_CK(cudaEventRecord(ev0_, s));
         MF3D_CK(cudaMemcpyAsync(x_.p, x0 ? x0 : x0_.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
         MF3D_CK(cudaMemsetAsync(tickets_.p, 0, tickets_.bytes, s));
-        pcg_init_kernel<<<1, 1, 0, s>>>(state_.as<PcgState>(), cfg_.cg_max_iter, cfg_.cg_check_every,
-                                        flexible_ ? 1 : 0, cfg_.cg_rtol, kSolveBudgetNs);
+        const bool mg = cfg_.solver == MF3D_SOLVER_MG, cg = cfg_.solver == MF3D_SOLVER_CG;
+        pcg_init_kernel<<<1, 1, 0, s>>>(state_.as<PcgState>(), mg ? cfg_.mg_max_cycles : cfg_.cg_max_iter,
+                                        mg ? 1 : cfg_.cg_check_every, (flexible_ && !cg) ? 1 : 0,
+                                        mg ? cfg_.rtol : cfg_.cg_rtol, kSolveBudgetNs, cfg_.solver);
         MF3D_LAUNCH_CK();
         launch_residual(s, 0);
         if (cfg_.use_graph) {
@@ -894,7 +920,8 @@ class HeadSolver {
             body_runs = -1; // known once the iteration count is back
         } else {
             // host-driven loop: one iteration per launch sequence, stop flag polled each time
-            for (int it = 0; it < std::max(cfg_.cg_max_iter, 1); ++it) {
+            const int cap = cfg_.solver == MF3D_SOLVER_MG ? cfg_.mg_max_cycles : cfg_.cg_max_iter;
+            for (int it = 0; it < std::max(cap, 1); ++it) {
                 record_body(s, false);
                 ++body_runs;
                 MF3D_CK(cudaMemcpyAsync(host_state_, state_.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
@@ -942,8 +969,10 @@ class HeadSolver {
         pcg_reopen_kernel<<<1, 1, 0, stream_>>>(st);
         MF3D_LAUNCH_CK();
         out.push_back(timing("matvec_dot", tm.mean_ms(reps, [&] {
-            matvec_dot_kernel<double><<<nb, PK_NT, 0, stream_>>>(op64_[0], p_.as<double>(), Ap_.as<double>(), st,
-                                                                 partials_.as<double>(), tickets_.as<unsigned>() + 3);
+            const ColLaunch cl = col_launch(G_[0].nx, G_[0].ny, G_[0].nz);
+            matvec_dot_kernel<double><<<cl.grid, cl.block, 0, stream_>>>(op64_[0], p_.as<double>(), Ap_.as<double>(),
+                                                                         st, partials_.as<double>(),
+                                                                         tickets_.as<unsigned>() + 3, cl.zchunk);
             MF3D_LAUNCH_CK();
         }), 40.0 * nd, 1));
         out.push_back(timing("residual_true", tm.mean_ms(reps, [&] { launch_residual(stream_, 1); }), 48.0 * nd, 0));
@@ -976,38 +1005,63 @@ class HeadSolver {
     void launch_residual(cudaStream_t s, int mode) {
         const size_t n = G_[0].n;
         double* out = mode == 0 ? r_.as<double>() : Ap_.as<double>();
-        residual_kernel<double><<<grid1d(n, PK_NT), PK_NT, 0, s>>>(
+        (void)n;
+        const ColLaunch cl = col_launch(G_[0].nx, G_[0].ny, G_[0].nz);
+        residual_kernel<double><<<cl.grid, cl.block, 0, s>>>(
             op64_[0], x_.as<double>(), b_.as<double>(), out, state_.as<PcgState>(), partials_.as<double>(),
             tickets_.as<unsigned>() + 2, mode, cfg_.conv_norm == MF3D_CONV_B ? 1 : 0,
-            mode == 0 ? r32_.as<float>() : nullptr);
+            mode == 1 ? nullptr : r32_.as<float>(), cond_, 0, cl.zchunk);
         MF3D_LAUNCH_CK();
     }
 
-    // One PCG iteration (loop body).
+    // One iteration (loop body) of the configured solver.
     void record_body(cudaStream_t s, bool with_cond) {
         const size_t n = G_[0].n;
         PcgState* st = state_.as<PcgState>();
-        vc_->run(s, z_.p, &st->rho_new);
         const unsigned nb = grid1d(n, PK_NT);
-        if (vc_->z_elt() == sizeof(double)) {
-            pupdate_kernel<double><<<nb, PK_NT, 0, s>>>(n, z_.as<double>(), p_.as<double>(), st);
+        const bool z64 = vc_->z_elt() == sizeof(double);
+        if (cfg_.solver == MF3D_SOLVER_MG) {
+            // v_cycle_recursive on (x, b) = x + V-cycle(b - A x) for the affine smoother
+            vc_->run(s, z_.p, nullptr);
+            if (z64) mg_xupdate_kernel<double><<<nb, PK_NT, 0, s>>>(n, x_.as<double>(), z_.as<double>(), st);
+            else mg_xupdate_kernel<float><<<nb, PK_NT, 0, s>>>(n, x_.as<double>(), z_.as<float>(), st);
+            MF3D_LAUNCH_CK();
+            const ColLaunch cl = col_launch(G_[0].nx, G_[0].ny, G_[0].nz);
+            residual_kernel<double><<<cl.grid, cl.block, 0, s>>>(op64_[0], x_.as<double>(), b_.as<double>(),
+                                                                 r_.as<double>(), st, partials_.as<double>(),
+                                                                 tickets_.as<unsigned>() + 2, 2,
+                                                                 cfg_.conv_norm == MF3D_CONV_B ? 1 : 0,
+                                                                 r32_.as<float>(), cond_, with_cond ? 1 : 0, cl.zchunk);
+            MF3D_LAUNCH_CK();
+            return;
+        }
+        const bool cg = cfg_.solver == MF3D_SOLVER_CG;
+        if (!cg) vc_->run(s, z_.p, &st->rho_new);
+        if (cg || z64) {
+            const double* z = cg ? r_.as<double>() : z_.as<double>();
+            pupdate_kernel<double><<<nb, PK_NT, 0, s>>>(n, z, p_.as<double>(), st);
         } else {
             pupdate_kernel<float><<<nb, PK_NT, 0, s>>>(n, z_.as<float>(), p_.as<double>(), st);
         }
         MF3D_LAUNCH_CK();
-        matvec_dot_kernel<double><<<nb, PK_NT, 0, s>>>(op64_[0], p_.as<double>(), Ap_.as<double>(), st,
-                                                       partials_.as<double>(), tickets_.as<unsigned>() + 3);
+        {
+            const ColLaunch cl = col_launch(G_[0].nx, G_[0].ny, G_[0].nz);
+            matvec_dot_kernel<double><<<cl.grid, cl.block, 0, s>>>(op64_[0], p_.as<double>(), Ap_.as<double>(), st,
+                                                                   partials_.as<double>(), tickets_.as<unsigned>() + 3,
+                                                                   cl.zchunk);
+        }
         MF3D_LAUNCH_CK();
-        if (vc_->z_elt() == sizeof(double)) {
+        if (cg || z64) {
+            const double* z = cg ? r_.as<double>() : z_.as<double>();
             xr_update_kernel<double><<<nb, PK_NT, 0, s>>>(n, x_.as<double>(), p_.as<double>(), r_.as<double>(),
-                                                          Ap_.as<double>(), z_.as<double>(), st,
-                                                          partials_.as<double>(), tickets_.as<unsigned>() + 4,
-                                                          cond_, with_cond ? 1 : 0, r32_.as<float>());
+                                                          Ap_.as<double>(), z, st, partials_.as<double>(),
+                                                          tickets_.as<unsigned>() + 4, cond_, with_cond ? 1 : 0,
+                                                          r32_.as<float>());
         } else {
             xr_update_kernel<float><<<nb, PK_NT, 0, s>>>(n, x_.as<double>(), p_.as<double>(), r_.as<double>(),
-                                                         Ap_.as<double>(), z_.as<float>(), st,
-                                                         partials_.as<double>(), tickets_.as<unsigned>() + 4,
-                                                         cond_, with_cond ? 1 : 0, r32_.as<float>());
+                                                         Ap_.as<double>(), z_.as<float>(), st, partials_.as<double>(),
+                                                         tickets_.as<unsigned>() + 4, cond_, with_cond ? 1 : 0,
+                                                         r32_.as<float>());
         }
         MF3D_LAUNCH_CK();
     }
@@ -1255,12 +1309,14 @@ static void run_velocity(const mf3d_grid* g, const mf3d_bc* bc, const double* h,
     const size_t n = (size_t)g->nx * g->ny * g->nz;
     VelOut o{U, V, W, layout};
     if (!out_host) {
-        velocity_kernel<<<grid1d(n, VEL_NT), VEL_NT, 0, s>>>(g->nx, g->ny, g->nz, g->dx, h, K, to_dev(*bc), o,
-                                                             nullptr, nullptr, nullptr, nullptr);
+        const ColLaunch cl = col_launch(g->nx, g->ny, g->nz);
+        velocity_kernel<<<cl.grid, cl.block, 0, s>>>(g->nx, g->ny, g->nz, g->dx, h, K, to_dev(*bc), o, nullptr, nullptr,
+                                                     nullptr, nullptr, cl.zchunk);
         MF3D_LAUNCH_CK();
         return;
     }
-    const unsigned nb = grid1d(n, VEL_NT);
+    const ColLaunch cl = col_launch(g->nx, g->ny, g->nz);
+    const unsigned nb = cl.nblocks;
     DevMem scratch((size_t)nb * 2 * sizeof(double) + 64);
     char* base = scratch.as<char>();
     unsigned long long* mx = (unsigned long long*)base;
@@ -1268,7 +1324,8 @@ static void run_velocity(const mf3d_grid* g, const mf3d_bc* bc, const double* h,
     double* sums = (double*)(base + 16);
     double* partials = (double*)(base + 64);
     MF3D_CK(cudaMemsetAsync(base, 0, 64, s));
-    velocity_kernel<<<nb, VEL_NT, 0, s>>>(g->nx, g->ny, g->nz, g->dx, h, K, to_dev(*bc), o, mx, partials, ticket, sums);
+    velocity_kernel<<<cl.grid, cl.block, 0, s>>>(g->nx, g->ny, g->nz, g->dx, h, K, to_dev(*bc), o, mx, partials, ticket,
+                                                 sums, cl.zchunk);
     MF3D_LAUNCH_CK();
     unsigned long long hb[4];
     MF3D_CK(cudaMemcpyAsync(hb, base, 32, cudaMemcpyDeviceToHost, s));
@@ -1435,7 +1492,9 @@ int mf3d_coarsen_K(const mf3d_grid* c, const double* Kf, double* Kc, void* strea
         need(Kc, "K_coarse");
         cudaStream_t s = (cudaStream_t)stream;
         const size_t n = (size_t)c->nx * c->ny * c->nz;
-        coarsen_kernel<<<grid1d(n, 256), 256, 0, s>>>(c->nx, c->ny, c->nz, Kf, Kc);
+        (void)n;
+        const ColLaunch cl = col_launch(c->nx, c->ny, c->nz);
+        coarsen_kernel<<<cl.grid, cl.block, 0, s>>>(c->nx, c->ny, c->nz, Kf, Kc, cl.zchunk);
         MF3D_LAUNCH_CK();
         MF3D_CK(cudaStreamSynchronize(s));
     });
@@ -1449,7 +1508,9 @@ int mf3d_build_rhs(const mf3d_grid* g, const mf3d_bc* bc, const double* K, doubl
         need(b, "b");
         cudaStream_t s = (cudaStream_t)stream;
         const size_t n = (size_t)g->nx * g->ny * g->nz;
-        rhs_guess_kernel<<<grid1d(n, 256), 256, 0, s>>>(g->nx, g->ny, g->nz, g->dx, K, to_dev(*bc), b, nullptr);
+        (void)n;
+        const ColLaunch cl = col_launch(g->nx, g->ny, g->nz);
+        rhs_guess_kernel<<<cl.grid, cl.block, 0, s>>>(g->nx, g->ny, g->nz, g->dx, K, to_dev(*bc), b, nullptr, cl.zchunk);
         MF3D_LAUNCH_CK();
         MF3D_CK(cudaStreamSynchronize(s));
     });

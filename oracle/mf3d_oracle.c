@@ -543,6 +543,67 @@ int og_solve_head_mg(int nx, int ny, int nz, double dx, const og_bc* bc, int pin
     return 0;
 }
 
+/* Plain CG: solve_head with solver CG, src/physics/flow/solve_head.cu:135-180 and
+ * src/numerics/solvers/cg.cuh:14-171: CG on the negated (SPD) operator with rhs -b, x from
+ * init_head_guess; stop when ||r|| <= rtol ||r0|| at every check_every-th iteration.  The
+ * iterates equal those of CG on A with b (r and p flip sign, alpha is unchanged). */
+int og_solve_head_cg(int nx, int ny, int nz, double dx, const og_bc* bc, int pin_mode, int max_iter,
+                     int check_every, double rtol, const double* K, double* h, og_result* res) {
+    const size_t n = (size_t)nx * ny * nz;
+    int has_dir = 0;
+    for (int f = 0; f < 6; ++f) has_dir |= (bc->type[f] == OG_DIRICHLET);
+    const int pin = pin_mode == 1 ? 1 : (pin_mode == 2 ? 0 : !has_dir);
+    double* b = (double*)malloc(n * sizeof(double));
+    double* r = (double*)malloc(n * sizeof(double));
+    double* p = (double*)malloc(n * sizeof(double));
+    double* Ap = (double*)malloc(n * sizeof(double));
+    og_build_rhs(nx, ny, nz, dx, bc, K, b);
+    og_init_guess(nx, ny, nz, bc, h);
+    memset(res, 0, sizeof(*res));
+    /* r = (-b) - (-A) x  ==  -(b - A x) */
+    og_apply_A(nx, ny, nz, dx, bc, pin, K, h, Ap);
+    for (size_t i = 0; i < n; ++i) r[i] = -b[i] + Ap[i];
+    memcpy(p, r, n * sizeof(double));
+    double rr = og_dot(n, r, r);
+    const double r0 = sqrt(rr), tol = r0 * rtol;
+    res->initial_residual = r0;
+    if (r0 <= tol) {
+        res->converged = 1;
+        res->final_residual = r0;
+        goto done;
+    }
+    for (int it = 0; it < max_iter; ++it) {
+        og_apply_A(nx, ny, nz, dx, bc, pin, K, p, Ap);
+        for (size_t i = 0; i < n; ++i) Ap[i] = -Ap[i];
+        const double pAp = og_dot(n, p, Ap);
+        if ((it + 1) % check_every == 0 && (!(fabs(pAp) >= 1e-30) || !isfinite(pAp))) {
+            res->iterations = it + 1;
+            res->final_residual = -1.0;
+            goto done;
+        }
+        const double alpha = rr / pAp;
+        for (size_t i = 0; i < n; ++i) {
+            h[i] += alpha * p[i];
+            r[i] -= alpha * Ap[i];
+        }
+        const double rr_new = og_dot(n, r, r);
+        if ((it + 1) % check_every == 0 && sqrt(rr_new) <= tol) {
+            res->converged = 1;
+            res->iterations = it + 1;
+            res->final_residual = sqrt(rr_new);
+            goto done;
+        }
+        const double beta = rr_new / rr;
+        for (size_t i = 0; i < n; ++i) p[i] = r[i] + beta * p[i];
+        rr = rr_new;
+    }
+    res->iterations = max_iter;
+    res->final_residual = sqrt(rr);
+done:
+    free(b); free(r); free(p); free(Ap);
+    return 0;
+}
+
 /* ------------------------------------------------------------------------ */
 /* Face velocity.  src/physics/flow/velocity_from_head.cu:102-551             */
 /* layout 0: compact MAC (U (nx+1)*ny*nz, V nx*(ny+1)*nz, W nx*ny*(nz+1));     */

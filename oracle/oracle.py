@@ -82,6 +82,7 @@ def lib():
                                         C.POINTER(Result)]
         L.og_solve_head_mg.argtypes = [i, i, i, d, pbc, i, i, i, i, i, i, d, _dp, _dp,
                                        C.POINTER(Result)]
+        L.og_solve_head_cg.argtypes = [i, i, i, d, pbc, i, i, i, d, _dp, _dp, C.POINTER(Result)]
         L.og_velocity.argtypes = [i, i, i, d, pbc, _dp, _dp, i, _dp, _dp, _dp]
         L.og_mass_balance.argtypes = [i, i, i, d, _dp, _dp, _dp, C.c_void_p, _dp]
         L.og_lnk_eval.argtypes = [i, i, i, d, i, _dp, _dp, _dp, _dp, _dp, d, _dp]
@@ -195,6 +196,16 @@ def solve_head_mg(K, bc, mg_levels, pre=2, post=2, coarse_iters=50, max_cycles=2
     res = Result()
     lib().og_solve_head_mg(*_dims(K), dx, C.byref(bc), pin_mode, mg_levels, pre, post,
                            coarse_iters, max_cycles, rtol, K.ravel(), h.ravel(), C.byref(res))
+    return h, res
+
+
+def solve_head_cg(K, bc, max_iter=1000, check_every=10, rtol=1e-8, dx=1.0, pin_mode=0):
+    """solve_head(CG): unpreconditioned CG from the x-linear guess.  Returns (h, Result)."""
+    K = _c(K)
+    h = np.empty_like(K)
+    res = Result()
+    lib().og_solve_head_cg(*_dims(K), dx, C.byref(bc), pin_mode, max_iter, check_every, rtol,
+                           K.ravel(), h.ravel(), C.byref(res))
     return h, res
 
 

@@ -114,6 +114,26 @@ def make_solve_cases():
         print("wrote", name, it, conv, r0, rf)
 
 
+OTHER_SOLVERS = [
+    # name, shape, sigma, solver (1 MG, 2 CG), levels, tol, check_every, max
+    ("mg_baseline16", (16, 16, 16), 1.0, 1, 3, 1e-9, 1, 60),
+    ("cg_baseline16", (16, 16, 16), 0.5, 2, 3, 1e-8, 1, 600),
+]
+
+
+def make_other_solver_cases():
+    bc = O.baseline_bc()
+    for name, shape, sigma, solver, levels, tol, ce, mx in OTHER_SOLVERS:
+        rng = np.random.default_rng(zlib.crc32(name.encode()))
+        K = lognormal(rng, shape, sigma)
+        h, it, conv, r0, rf = O.ref_solve_head(K, bc, levels, solver=solver, mg_max_cycles=mx, max_iter=mx,
+                                               check_every=ce, cg_rtol=tol, rtol=tol)
+        np.savez_compressed(os.path.join(OUT, f"{name}.npz"), K=K, h=h,
+                            info=np.array([it, int(conv), levels, ce, mx, solver]),
+                            res=np.array([r0, rf, tol]))
+        print("wrote", name, it, conv, r0, rf)
+
+
 if __name__ == "__main__":
     if "--out" in sys.argv:
         OUT = sys.argv[sys.argv.index("--out") + 1]
@@ -124,3 +144,4 @@ if __name__ == "__main__":
     make_transfer_cases()
     make_vcycle_cases()
     make_solve_cases()
+    make_other_solver_cases()

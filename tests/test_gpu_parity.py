@@ -250,3 +250,41 @@ def test_kfield_vs_oracle(mf3d, oracle_mod):
     assert np.abs(_np(lnk) - ref).max() < 1e-9
     K = M.generate_K_field(g, 2.0, (4.0, 4.0, 2.0), seed=99)
     assert np.allclose(_np(K), np.exp(ref), rtol=1e-9)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_standalone_mg_solver_vs_oracle(mf3d, oracle_mod, prec):
+    """solver = mg: V-cycles on the current head until ||r||/||r0|| < rtol
+    (mg_solve, src/multigrid/cycle/v_cycle.cu:76-116)."""
+    M, O = mf3d, oracle_mod
+    shape = (32, 32, 32)
+    K = _lognormal(shape, 1.0, 21)
+    g = M.Grid3D(32, 32, 32, 1.0)
+    cfg = M.HeadSolveConfig(solver_type=M.SOLVER_MG, mg_levels=4, mg_max_cycles=60, rtol=1e-10,
+                            precision=prec)
+    s = M.HeadSolver(g, M.BCSpec.darcy_x(), cfg)
+    s.set_K(_t(K))
+    h = _t(np.zeros(shape))
+    res = s.solve(h)
+    ho, ro = O.solve_head_mg(K, O.baseline_bc(), 4, max_cycles=60, rtol=1e-10)
+    assert res.converged and ro.converged
+    if prec == 0:
+        assert abs(res.num_iterations - ro.iterations) <= 1
+    assert _rel(_np(h), ho) < 1e-8
+
+
+def test_plain_cg_solver_vs_oracle(mf3d, oracle_mod):
+    """solver = cg: unpreconditioned CG (cg_solve, src/numerics/solvers/cg.cuh:14-171)."""
+    M, O = mf3d, oracle_mod
+    shape = (16, 16, 16)
+    K = _lognormal(shape, 0.5, 22)
+    g = M.Grid3D(16, 16, 16, 1.0)
+    cfg = M.HeadSolveConfig(solver_type=M.SOLVER_CG, cg_max_iter=800, cg_check_every=1, cg_rtol=1e-9)
+    s = M.HeadSolver(g, M.BCSpec.darcy_x(), cfg)
+    s.set_K(_t(K))
+    h = _t(np.zeros(shape))
+    res = s.solve(h)
+    ho, ro = O.solve_head_cg(K, O.baseline_bc(), max_iter=800, check_every=1, rtol=1e-9)
+    assert res.converged and ro.converged
+    assert abs(res.num_iterations - ro.iterations) <= 2
+    assert _rel(_np(h), ho) < 1e-7

@@ -119,3 +119,21 @@ def test_live_reference_64cubed(mf3d, oracle_mod):
     U, V, W = _t(np.zeros(su)), _t(np.zeros(sv)), _t(np.zeros(sw))
     M.compute_velocity_from_head(U, V, W, h, K, g, M.BCSpec.darcy_x())
     assert _rel(_np(U), Ur.ravel()) < 1e-9
+
+
+@pytest.mark.parametrize("path", _files("mg_") + _files("cg_"), ids=os.path.basename)
+def test_other_solvers_match_reference_golden(mf3d, path):
+    M = mf3d
+    z = np.load(path)
+    it, conv, levels, ce, mx, solver = (int(v) for v in z["info"])
+    r0, rf, tol = (float(v) for v in z["res"])
+    nz, ny, nx = z["K"].shape
+    cfg = M.HeadSolveConfig(solver_type=solver, mg_levels=levels, mg_max_cycles=mx, rtol=tol,
+                            cg_max_iter=mx, cg_check_every=ce, cg_rtol=tol)
+    s = M.HeadSolver(M.Grid3D(nx, ny, nz, 1.0), M.BCSpec.darcy_x(), cfg)
+    s.set_K(_t(z["K"]))
+    h = _t(np.zeros(z["K"].shape))
+    res = s.solve(h)
+    assert res.converged == bool(conv)
+    assert abs(res.num_iterations - it) <= (1 if solver == 1 else 2)
+    assert _rel(_np(h), z["h"]) < 1e-8

@@ -72,3 +72,18 @@ def test_oracle_pcg_matches_reference(oracle_mod, path):
     assert abs(res.iterations - it) <= (1 if ce == 1 else 0)
     assert abs(res.initial_residual - r0) < 1e-12 * r0
     assert _rel(h, z["h"]) < 1e-9
+
+
+@pytest.mark.parametrize("path", _files("mg_") + _files("cg_"), ids=os.path.basename)
+def test_oracle_other_solvers_match_reference(oracle_mod, path):
+    O = oracle_mod
+    z = np.load(path)
+    it, conv, levels, ce, mx, solver = (int(v) for v in z["info"])
+    r0, rf, tol = (float(v) for v in z["res"])
+    if solver == 1:
+        h, res = O.solve_head_mg(z["K"], O.baseline_bc(), levels, max_cycles=mx, rtol=tol)
+    else:
+        h, res = O.solve_head_cg(z["K"], O.baseline_bc(), max_iter=mx, check_every=ce, rtol=tol)
+    assert bool(res.converged) == bool(conv)
+    assert abs(res.iterations - it) <= 1
+    assert _rel(h, z["h"]) < 1e-8
