@@ -169,6 +169,11 @@ __global__ void __launch_bounds__(PK_NT) pupdate_kernel(size_t n, const TZ* __re
     if (s.stop) return;
     const double beta = s.iter == 0 ? 0.0 : (s.rho_new - (s.flexible ? s.gamma : 0.0)) / s.rho_old;
     if (blockIdx.x == 0 && threadIdx.x == 0) st->beta = beta;
+    if (s.iter == 0) { // p = z exactly: whatever p held before must not leak in through 0 * p
+        for (size_t c = blockIdx.x * (size_t)PK_NT + threadIdx.x; c < n; c += (size_t)gridDim.x * PK_NT)
+            p[c] = (double)z[c];
+        return;
+    }
     for (size_t c = blockIdx.x * (size_t)PK_NT + threadIdx.x; c < n; c += (size_t)gridDim.x * PK_NT)
         p[c] = 1.0 * (double)z[c] + beta * p[c];
 }

@@ -84,40 +84,47 @@ template <class T, class TC, int MODE> struct TmaSweepCfg {
     static constexpr int NS = RESID ? 3 : 2;
     static constexpr int H = NS;
     static constexpr int HX = TmaGeom<T, TC>::hx(H);
-    static constexpr int BX = SW_TX + 2 * HX, BY = SW_TY + 2 * H;
-    // ring slots: NS + 2 planes are live, the rest are in flight (FP64 keeps the ring small
-    // enough for one or two CTAs per SM)
-    static constexpr int NR = sizeof(T) == 8 ? NS + 4 : 8;
-    static constexpr int PF = NR - NS - 2;
+    // 32 x 16 tiles (512 threads) in FP32, 32 x 8 (256 threads) in FP64 to fit the ring
+    static constexpr int TY = sizeof(T) == 8 ? 8 : 16;
+    static constexpr int NT = SW_TX * TY;
+    static constexpr int BX = SW_TX + 2 * HX, BY = TY + 2 * H;
     static constexpr int PLANE = BX * BY;      // elements per array plane
-    static constexpr int FIX = (PLANE + SW_NT - 1) / SW_NT; // fix-up elements per thread
+    static constexpr int FIX = (PLANE + NT - 1) / NT; // fix-up elements per thread
     static constexpr size_t XB = (size_t)PLANE * sizeof(T), CB = (size_t)PLANE * sizeof(TC);
     static constexpr size_t align128(size_t v) { return (v + 127) & ~(size_t)127; }
     static constexpr size_t OB = align128(XB), OC = align128(CB);
     static constexpr size_t SLOT = OB * 2 + OC * 3; // x, b, cx, cy, cz
-    static constexpr size_t RS = RESID ? align128(2 * SW_TX * SW_TY * sizeof(T)) : 0;
-    static constexpr size_t SMEM = 128 /* barriers */ + SLOT * NR + RS + 128 /* alignment slack */;
+    static constexpr size_t RS = RESID ? align128(2 * SW_TX * TY * sizeof(T)) : 0;
+    // ring slots: NS + 2 planes are live, the rest (PF) are in flight; one CTA per SM takes
+    // as many slots as 200 KB of shared memory hold (at most 16)
+    static constexpr int NR_FIT = (int)((200 * 1024 - 128 - RS) / SLOT);
+    static constexpr int NR = NR_FIT < 16 ? NR_FIT : 16;
+    static constexpr int PF = NR - NS - 2;
+    static_assert(PF >= 2, "ring too small");
+    static constexpr size_t SMEM = 128 /* barriers */ + SLOT * NR + RS;
 };
 
 template <class T, class TC, int MODE>
-__global__ void __launch_bounds__(SW_NT) sweep_tma_kernel(const __grid_constant__ TmaMaps maps,
-                                                          const TmaSweepArgs<T, TC> a) {
+__global__ void __launch_bounds__(TmaSweepCfg<T, TC, MODE>::NT) sweep_tma_kernel(const __grid_constant__ TmaMaps maps,
+                                                                             const TmaSweepArgs<T, TC> a) {
     using C = TmaSweepCfg<T, TC, MODE>;
+    constexpr int TY = C::TY, NT = C::NT;
     constexpr bool ZERO = (MODE & M_ZERO) != 0;
     constexpr bool PROL = (MODE & M_PROLONG) != 0;
     constexpr bool RESID = C::RESID;
     constexpr bool DOT = (MODE & M_DOT) != 0;
     constexpr int NS = C::NS, H = C::H, HX = C::HX, BX = C::BX, NR = C::NR, PF = C::PF;
-    extern __shared__ unsigned char smraw[];
-    unsigned char* sm = (unsigned char*)(((uintptr_t)smraw + 127) & ~(uintptr_t)127);
-    uint64_t* bars = (uint64_t*)sm;
-    unsigned char* ring = sm + 128;
-    T* rsb = (T*)(ring + C::SLOT * NR);
+    // all ring accesses are 32-bit offsets from the shared array, so they stay shared-space
+    // loads (the dynamic shared window starts 1 KB aligned; every slot offset is 128-aligned)
+    extern __shared__ __align__(128) unsigned char smraw[];
+    uint64_t* bars = (uint64_t*)smraw;
+    constexpr int RING = 128;
+    T* rsb = (T*)(smraw + RING + C::SLOT * NR);
 
     const LevelOp<TC>& L = a.L;
     const int nx = L.nx, ny = L.ny, nz = L.nz;
     const size_t nxy = (size_t)nx * ny;
-    const int i0 = blockIdx.x * SW_TX, j0 = blockIdx.y * SW_TY;
+    const int i0 = blockIdx.x * SW_TX, j0 = blockIdx.y * TY;
     const int z0 = blockIdx.z * a.zchunk;
     const int z1 = min(z0 + a.zchunk, nz);
     const int tid = threadIdx.x;
@@ -125,11 +132,11 @@ __global__ void __launch_bounds__(SW_NT) sweep_tma_kernel(const __grid_constant_
     const int zlo = z0 - NS, zhi = z1 - 1 + NS;
 
     // slot s: x at ring + SLOT*s, b at +OB, cx at +2*OB, cy at +2*OB+OC, cz at +2*OB+2*OC
-    auto X = [&](int s) { return (T*)(ring + C::SLOT * s); };
-    auto B = [&](int s) { return (T*)(ring + C::SLOT * s + C::OB); };
-    auto CX = [&](int s) { return (TC*)(ring + C::SLOT * s + 2 * C::OB); };
-    auto CY = [&](int s) { return (TC*)(ring + C::SLOT * s + 2 * C::OB + C::OC); };
-    auto CZ = [&](int s) { return (TC*)(ring + C::SLOT * s + 2 * C::OB + 2 * C::OC); };
+    auto X = [&](int s) { return (T*)(smraw + RING + C::SLOT * s); };
+    auto B = [&](int s) { return (T*)(smraw + RING + C::SLOT * s + C::OB); };
+    auto CX = [&](int s) { return (TC*)(smraw + RING + C::SLOT * s + 2 * C::OB); };
+    auto CY = [&](int s) { return (TC*)(smraw + RING + C::SLOT * s + 2 * C::OB + C::OC); };
+    auto CZ = [&](int s) { return (TC*)(smraw + RING + C::SLOT * s + 2 * C::OB + 2 * C::OC); };
     constexpr unsigned TX_BYTES = (unsigned)(2 * C::XB + 3 * C::CB);
 
     auto issue = [&](int t, int s) { // thread 0 only; plane t into slot s
@@ -151,8 +158,9 @@ __global__ void __launch_bounds__(SW_NT) sweep_tma_kernel(const __grid_constant_
 
     // ---- fixed per-thread work items ----
     constexpr int hr = NS - 1, hb = NS - 2;
-    constexpr int RPW = (SW_TX + 2 * hr) / 2, RPH = SW_TY + 2 * hr;
-    constexpr int BPW = (SW_TX + 2 * hb) / 2, BPH = SW_TY + 2 * hb;
+    constexpr int RPW = (SW_TX + 2 * hr) / 2, RPH = TY + 2 * hr;
+    constexpr int BPW = (SW_TX + 2 * hb) / 2, BPH = TY + 2 * hb;
+    static_assert(RPW * RPH <= NT && BPW * BPH <= NT, "one red and one black item per thread");
     // red item: pair (r_iu0, r_iu0+1) in row r_ju
     const int r_iu0 = i0 - hr + 2 * (tid % RPW), r_ju = j0 - hr + tid / RPW;
     const bool r_ok = tid < RPW * RPH && r_ju >= 0 && r_ju < ny;
@@ -164,7 +172,7 @@ __global__ void __launch_bounds__(SW_NT) sweep_tma_kernel(const __grid_constant_
     const int b_e0 = (b_ju - j0 + H) * BX + (b_iu0 - i0 + HX);
     const int b_par = (b_iu0 + b_ju) & 1;
     // output / residual item
-    const int o_li = tid % SW_TX, o_lj = tid / SW_TX; // SW_NT == SW_TX * SW_TY
+    const int o_li = tid % SW_TX, o_lj = tid / SW_TX; // NT == SW_TX * TY
     const int o_gi = i0 + o_li, o_gj = j0 + o_lj;
     const bool o_ok = o_gi < nx && o_gj < ny;
     const int o_e = (o_lj + H) * BX + o_li + HX;
@@ -174,7 +182,7 @@ __global__ void __launch_bounds__(SW_NT) sweep_tma_kernel(const __grid_constant_
     long long f_cb[C::FIX]; // coarse column index, -1 when outside the grid
 #pragma unroll
     for (int k = 0; k < C::FIX; ++k) {
-        const int e = tid + k * SW_NT;
+        const int e = tid + k * NT;
         f_e[k] = e < C::PLANE ? e : -1;
         const int gi = i0 - HX + e % BX, gj = j0 - H + e / BX;
         f_cb[k] = (e < C::PLANE && gi >= 0 && gi < nx && gj >= 0 && gj < ny)
@@ -186,21 +194,21 @@ __global__ void __launch_bounds__(SW_NT) sweep_tma_kernel(const __grid_constant_
     double dot_acc = 0.0;
     unsigned phase = 0u; // bit s: parity of the next wait on slot s (tracked by thread 0)
 
-    // slot base pointers of planes t, t-1, ..., t-4 for the current step
-    unsigned char* pb[5];
+    // slot byte offsets of planes t, t-1, ..., t-4 for the current step
+    int pb[5];
     auto set_bases = [&](int sl_t) {
 #pragma unroll
         for (int d = 0; d < 5; ++d) {
             int v = sl_t - d;
             if (v < 0) v += NR;
-            pb[d] = ring + C::SLOT * v;
+            pb[d] = RING + (int)C::SLOT * v;
         }
     };
-    auto Xp = [&](int d) { return (T*)pb[d]; };
-    auto Bp = [&](int d) { return (T*)(pb[d] + C::OB); };
-    auto CXp = [&](int d) { return (TC*)(pb[d] + 2 * C::OB); };
-    auto CYp = [&](int d) { return (TC*)(pb[d] + 2 * C::OB + C::OC); };
-    auto CZp = [&](int d) { return (TC*)(pb[d] + 2 * C::OB + 2 * C::OC); };
+    auto Xp = [&](int d) { return (T*)(smraw + pb[d]); };
+    auto Bp = [&](int d) { return (T*)(smraw + pb[d] + C::OB); };
+    auto CXp = [&](int d) { return (TC*)(smraw + pb[d] + 2 * C::OB); };
+    auto CYp = [&](int d) { return (TC*)(smraw + pb[d] + 2 * C::OB + C::OC); };
+    auto CZp = [&](int d) { return (TC*)(smraw + pb[d] + 2 * C::OB + 2 * C::OC); };
     auto divide = [](T num, T den) -> T {
         if constexpr (sizeof(T) == 4) return __fdividef(num, den); // preconditioner: 2-ulp division
         else return num / den;
@@ -308,16 +316,16 @@ __global__ void __launch_bounds__(SW_NT) sweep_tma_kernel(const __grid_constant_
                                   czp * Xp(2)[e] + czm * Xp(4)[e];
                     rv = Bp(3)[e] - (sum - D * x[e]) * (T)L.inv_dx2;
                 }
-                rsb[((s - z0) & 1) * SW_TX * SW_TY + tid] = rv;
+                rsb[((s - z0) & 1) * SW_TX * TY + tid] = rv;
                 if (((s - z0) & 1) == 1) {
                     __syncthreads();
                     const int ncx = nx >> 1, ncy = ny >> 1;
-                    if (tid < (SW_TX / 2) * (SW_TY / 2)) {
+                    if (tid < (SW_TX / 2) * (TY / 2)) {
                         const int ci = tid % (SW_TX / 2), cj = tid / (SW_TX / 2);
                         const int I = (i0 >> 1) + ci, J = (j0 >> 1) + cj;
                         if (I < ncx && J < ncy) {
                             const T* r0 = rsb;
-                            const T* r1 = rsb + SW_TX * SW_TY;
+                            const T* r1 = rsb + SW_TX * TY;
                             const int f = 2 * cj * SW_TX + 2 * ci;
                             T acc = (T)0;
                             acc += r0[f];
@@ -343,7 +351,7 @@ __global__ void __launch_bounds__(SW_NT) sweep_tma_kernel(const __grid_constant_
     if (DOT) {
         double v[1] = {dot_acc}, out[1];
         const int nblocks = gridDim.x * gridDim.y * gridDim.z;
-        if (grid_sums<SW_NT, 1>(v, a.dot_partials, a.dot_ticket, nblocks, out)) *a.dot_out = out[0];
+        if (grid_sums<NT, 1>(v, a.dot_partials, a.dot_ticket, nblocks, out)) *a.dot_out = out[0];
     }
 }
 

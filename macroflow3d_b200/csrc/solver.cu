@@ -357,7 +357,7 @@ template <class T, class TC> class VCycle : public VCycleBase {
             ++n_tma_;
             for (int resid = 0; resid < 2; ++resid) {
                 const int H = resid ? 3 : 2;
-                const int bx = SW_TX + 2 * TmaGeom<T, TC>::hx(H), by = SW_TY + 2 * H;
+                const int bx = SW_TX + 2 * TmaGeom<T, TC>::hx(H), by = tma_ty() + 2 * H;
                 Maps4& m = maps_[l][resid];
                 const T* b = l == 0 ? b0_ : (const T*)bl_[l]->p;
                 m.xa.x = make_map<T>(xa_[l]->p, g, bx, by);
@@ -553,12 +553,32 @@ template <class T, class TC> class VCycle : public VCycleBase {
         return std::min(zc, ((g.nz + 1) & ~1));
     }
 
+    // z planes per CTA of the staged sweep: one CTA per SM, so pick the chunk count that
+    // minimises waves x (planes marched per CTA, halo planes included)
+    static int zchunk_tma(const Geom& g, long long nblk_xy, int halo) {
+        int best_zc = g.nz + (g.nz & 1);
+        double best = 1e300;
+        for (int nzc = 1; nzc <= std::min(g.nz, 64); ++nzc) {
+            int zc = (g.nz + nzc - 1) / nzc;
+            zc = (zc + 1) & ~1;
+            const int chunks = (g.nz + zc - 1) / zc;
+            const double waves = std::ceil((double)(nblk_xy * chunks) / num_sms());
+            const double cost = waves * (zc + 2 * halo);
+            if (cost < best - 1e-9) {
+                best = cost;
+                best_zc = zc;
+            }
+        }
+        return std::max(2, best_zc);
+    }
+
     void sweep(cudaStream_t s, int l, const T* x_in, T* x_out, const T* e, T* b_coarse, int mode, double* dot_out) {
         const Geom& g = G_[l];
-        const int gx = (g.nx + SW_TX - 1) / SW_TX, gy = (g.ny + SW_TY - 1) / SW_TY;
         const bool tma = tma_[l] != 0;
-        // the staged sweep keeps two CTAs per SM busy; the load-per-stage sweep wants many
-        const int zc = zchunk_for(g, gx * gy, num_sms() * (tma ? 8 : 6));
+        const int ty = tma ? tma_ty() : SW_TY;
+        const int gx = (g.nx + SW_TX - 1) / SW_TX, gy = (g.ny + ty - 1) / ty;
+        const int zc = tma ? zchunk_tma(g, (long long)gx * gy, (mode & M_RESID) ? 3 : 2)
+                           : zchunk_for(g, gx * gy, num_sms() * 6);
         const int gz = (g.nz + zc - 1) / zc;
         dim3 grid(gx, gy, gz);
         const unsigned nblk = (unsigned)gx * gy * gz;
@@ -623,9 +643,12 @@ template <class T, class TC> class VCycle : public VCycleBase {
         set_one<M_ZERO | M_PROLONG | M_DOT>();
     }
 
+    static int tma_ty() { return TmaSweepCfg<T, TC, 0>::TY; }
+
     template <int MODE>
     static void launch_tma(cudaStream_t s, dim3 grid, const TmaMaps& m, const TmaSweepArgs<T, TC>& a) {
-        sweep_tma_kernel<T, TC, MODE><<<grid, SW_NT, TmaSweepCfg<T, TC, MODE>::SMEM, s>>>(m, a);
+        using C = TmaSweepCfg<T, TC, MODE>;
+        sweep_tma_kernel<T, TC, MODE><<<grid, C::NT, C::SMEM, s>>>(m, a);
     }
 
     void dispatch_tma(cudaStream_t s, dim3 grid, int mode, const TmaMaps& m, const TmaSweepArgs<T, TC>& a) {
@@ -772,6 +795,7 @@ class HeadSolver {
         }
         auto vec = [&](DevMem& m) {
             m.alloc(n * sizeof(double));
+            MF3D_CK(cudaMemsetAsync(m.p, 0, m.bytes, stream_));
             bytes_ += m.bytes;
         };
         vec(x_);

@@ -74,16 +74,29 @@ def test_oracle_pcg_matches_reference(oracle_mod, path):
     assert _rel(h, z["h"]) < 1e-9
 
 
-@pytest.mark.parametrize("path", _files("mg_") + _files("cg_"), ids=os.path.basename)
-def test_oracle_other_solvers_match_reference(oracle_mod, path):
+@pytest.mark.parametrize("path", _files("mg_"), ids=os.path.basename)
+def test_oracle_mg_matches_reference(oracle_mod, path):
     O = oracle_mod
     z = np.load(path)
     it, conv, levels, ce, mx, solver = (int(v) for v in z["info"])
     r0, rf, tol = (float(v) for v in z["res"])
-    if solver == 1:
-        h, res = O.solve_head_mg(z["K"], O.baseline_bc(), levels, max_cycles=mx, rtol=tol)
-    else:
-        h, res = O.solve_head_cg(z["K"], O.baseline_bc(), max_iter=mx, check_every=ce, rtol=tol)
+    h, res = O.solve_head_mg(z["K"], O.baseline_bc(), levels, max_cycles=mx, rtol=tol)
     assert bool(res.converged) == bool(conv)
     assert abs(res.iterations - it) <= 1
     assert _rel(h, z["h"]) < 1e-8
+
+
+@pytest.mark.parametrize("path", _files("cg_"), ids=os.path.basename)
+def test_reference_cg_defect_is_recorded(oracle_mod, path):
+    """The reference's solver=cg path does not converge: cg_solve captures the d_rr / d_rr_new
+    spans before its loop (src/numerics/solvers/cg.cuh:29-30) and then swaps the buffers
+    (cg.cuh:156), so alpha keeps using ||r0||^2 and the reported residual is ||r0||.  The
+    golden run shows exactly that; CG as documented (the oracle, and this library) converges."""
+    O = oracle_mod
+    z = np.load(path)
+    it, conv, levels, ce, mx, solver = (int(v) for v in z["info"])
+    r0, rf, tol = (float(v) for v in z["res"])
+    assert solver == 2 and not conv and it == mx and rf == r0
+    h, res = O.solve_head_cg(z["K"], O.baseline_bc(), max_iter=mx, check_every=ce, rtol=tol)
+    assert res.converged and res.iterations < mx
+    assert abs(res.initial_residual - r0) < 1e-12 * r0
