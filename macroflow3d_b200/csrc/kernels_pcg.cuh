@@ -25,12 +25,13 @@ struct PcgState {
     double alpha, beta;
     int iter, max_iter, check_every, flexible;
     int converged, status, stop, body_count;
-    int solver;                    // 0 PCG (preconditioned), 1 plain CG, 2 standalone MG
+    int solver;                    // MF3D_SOLVER_*: 0 PCG_MG, 1 standalone MG, 2 plain CG
     unsigned long long t_start_ns; // %globaltimer at the start of the solve
     unsigned long long budget_ns;  // device-time limit of one solve
 };
 
 enum : int { PCG_OK = 0, PCG_BREAKDOWN = 1, PCG_NONFINITE = 2, PCG_TIMEOUT = 3 };
+enum : int { SOLVE_PCG_MG = 0, SOLVE_MG = 1, SOLVE_CG = 2 }; // the ABI's MF3D_SOLVER_* codes
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -79,7 +80,7 @@ __global__ void __launch_bounds__(PK_NT) residual_kernel(const LevelOp<TC> L, co
                                                          PcgState* st, double* partials, unsigned* ticket,
                                                          int mode, int ref_is_b, float* __restrict__ r32,
                                                          cudaGraphConditionalHandle cond, int use_cond, int zchunk) {
-    const bool mg = st->solver == 2;
+    const bool mg = st->solver == SOLVE_MG;
     const bool first = first_thread();
     if (mode == 2 && st->stop) { // standalone MG: finished before this cycle
         if (use_cond && first) cudaGraphSetConditional(cond, 0u);
@@ -122,16 +123,16 @@ __global__ void __launch_bounds__(PK_NT) residual_kernel(const LevelOp<TC> L, co
             st->status = PCG_OK;
             st->rho_new = st->rho_old = st->gamma = st->pAp = 0.0;
             st->alpha = st->beta = 0.0;
-            if (st->solver == 2) {
+            if (st->solver == SOLVE_MG) {
                 // mg_solve has no early exit (src/multigrid/cycle/v_cycle.cu:90-113)
                 st->stop = st->max_iter <= 0 ? 1 : 0;
             } else {
                 // the reference returns at once when ||r0|| is (near) zero (pcg.cuh:122-127, cg.cuh:61-66)
                 const double r0 = sqrt(out[0]);
-                const bool done = st->solver == 1 ? r0 <= st->rtol * r0 : r0 < 1e-15;
+                const bool done = st->solver == SOLVE_CG ? r0 <= st->rtol * r0 : r0 < 1e-15;
                 st->stop = (done || st->max_iter <= 0) ? 1 : 0;
                 if (done) st->converged = 1;
-                st->rho_new = st->solver == 1 ? out[0] : 0.0; // plain CG: rho = <r, r>
+                st->rho_new = st->solver == SOLVE_CG ? out[0] : 0.0; // plain CG: rho = <r, r>
             }
             if (!isfinite(out[0])) { st->status = PCG_NONFINITE; st->stop = 1; }
             st->t_start_ns = global_ns();
@@ -243,7 +244,7 @@ __global__ void __launch_bounds__(PK_NT) xr_update_kernel(size_t n, double* __re
         st->rr = out[0];
         st->gamma = out[1];
         st->rho_old = s.rho_new;
-        if (s.solver == 1) st->rho_new = out[0]; // plain CG: rho = <r, r> for the next beta
+        if (s.solver == SOLVE_CG) st->rho_new = out[0]; // plain CG: rho = <r, r> for the next beta
         int stop = 0;
         if (!isfinite(out[0]) || !isfinite(s.pAp) || !isfinite(alpha)) {
             st->status = PCG_NONFINITE;
@@ -256,7 +257,7 @@ __global__ void __launch_bounds__(PK_NT) xr_update_kernel(size_t n, double* __re
             const double rn = sqrt(out[0]);
             st->final_res = rn;
             // pcg.cuh:158-160 tests ||r||/||r0|| < rtol; cg.cuh:142-150 tests ||r|| <= rtol ||r0||
-            if (s.solver == 1 ? rn <= s.rtol * s.ref_norm : rn / s.ref_norm < s.rtol) {
+            if (s.solver == SOLVE_CG ? rn <= s.rtol * s.ref_norm : rn / s.ref_norm < s.rtol) {
                 st->converged = 1;
                 stop = 1;
             }
