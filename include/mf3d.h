@@ -166,6 +166,20 @@ int mf3d_velocity_mass_balance(const mf3d_grid* grid, const mf3d_bc* bc, const d
                                const double* K_dev, double* U_dev, double* V_dev, double* W_dev,
                                double* out_host, void* stream);
 
+/* No counterpart in the reference.  Same results as mf3d_velocity_mass_balance, but its
+ * reduction scratch is a static device array (64 B + 16 B per block, 262,208 B in all), so it
+ * allocates and frees no device memory: for callers whose device memory is fully owned by
+ * another allocator, and for callers that cannot afford the implicit device-wide
+ * synchronisation of cudaFree.  Limit: at most MF3D_MB_NOALLOC_MAX_BLOCKS reduction blocks,
+ * i.e. ceil(nx/32) * ceil(ny/8) <= 16384; larger grids return MF3D_E_INVALID.  The device
+ * address of the array is looked up on the first call on each device, so on each device that
+ * first call should come before any stream capture.  Calls that overlap on one device share
+ * the array and race: serialise them. */
+#define MF3D_MB_NOALLOC_MAX_BLOCKS 16384
+int mf3d_velocity_mass_balance_noalloc(const mf3d_grid* grid, const mf3d_bc* bc, const double* h_dev,
+                                       const double* K_dev, double* U_dev, double* V_dev,
+                                       double* W_dev, double* out_host, void* stream);
+
 /* ---- operator pieces (device pointers, FP64; in-place where the reference is) ------------- */
 /* VarCoeffLaplacian::apply, src/numerics/operators/varcoeff_laplacian.cu:241-277 */
 int mf3d_apply_A(const mf3d_grid* g, const mf3d_bc* bc, int pin, const double* K, const double* x,

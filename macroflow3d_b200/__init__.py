@@ -22,6 +22,7 @@ PREC_FP64, PREC_FP32, PREC_BF16 = 0, 1, 2
 CONV_R0, CONV_B = 0, 1
 VEL_COMPACT, VEL_PADDED = 0, 1
 COV_EXPONENTIAL, COV_GAUSSIAN = 0, 1
+MB_NOALLOC_MAX_BLOCKS = 16384
 
 
 @dataclass
@@ -275,6 +276,20 @@ def velocity_mass_balance(U, V, W, h, K, grid: Grid3D, bc: BCSpec) -> Tuple[floa
     check(lib().mf3d_velocity_mass_balance(C.byref(grid.c()), C.byref(_bc(bc)), _f64(h, n, "h"),
                                            _f64(K, n, "K"), _f64(U, su, "U"), _f64(V, sv, "V"),
                                            _f64(W, sw, "W"), out, _stream()))
+    return out[0], out[1], out[2]
+
+
+def velocity_mass_balance_noalloc(U, V, W, h, K, grid: Grid3D,
+                                  bc: BCSpec) -> Tuple[float, float, float]:
+    """velocity_mass_balance without device allocation: the reduction scratch is a static
+    device array (at most MB_NOALLOC_MAX_BLOCKS reduction blocks).  Calls that overlap on one
+    device race on that array."""
+    n = grid.num_cells()
+    su, sv, sw = velocity_sizes(grid, VEL_COMPACT)
+    out = (C.c_double * 3)()
+    check(lib().mf3d_velocity_mass_balance_noalloc(
+        C.byref(grid.c()), C.byref(_bc(bc)), _f64(h, n, "h"), _f64(K, n, "K"),
+        _f64(U, su, "U"), _f64(V, sv, "V"), _f64(W, sw, "W"), out, _stream()))
     return out[0], out[1], out[2]
 
 

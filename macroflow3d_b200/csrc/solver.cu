@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -1373,6 +1374,79 @@ int mf3d_velocity_mass_balance(const mf3d_grid* g, const mf3d_bc* bc, const doub
     return guard([&] {
         need(out_host, "out_host");
         run_velocity(g, bc, h, K, MF3D_VEL_COMPACT, U, V, W, out_host, (cudaStream_t)stream);
+    });
+}
+
+// ---- mass balance with static scratch (no device allocation) -------------------------------
+// The reduction scratch of the fused velocity + mass-balance kernel (max bits, ticket, two
+// sums, then two partial sums per block) lives in one file-scope device array, so this entry
+// point calls neither cudaMalloc nor cudaFree.  One array exists per device: calls that
+// overlap on the same device (two streams or two host threads) share it and race.
+namespace {
+constexpr unsigned kMbNoAllocMaxBlocks = MF3D_MB_NOALLOC_MAX_BLOCKS;
+constexpr size_t kMbNoAllocHeader = 64;
+constexpr size_t kMbNoAllocBytes = kMbNoAllocHeader + (size_t)kMbNoAllocMaxBlocks * 2 * sizeof(double);
+static __device__ __align__(256) unsigned char g_mb_scratch[kMbNoAllocBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mb_mu;
+unsigned char* g_mb_ptr[kMaxDevices] = {};
+
+// Device address of g_mb_scratch on the current device, looked up once per device with that
+// device current.  The first call on a device does the lookup (which may load the module on
+// that device), so on each device that first call should come before any stream capture.
+unsigned char* mb_scratch_on_current_device() {
+    int dev = 0;
+    MF3D_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) throw Error(MF3D_E_INVALID, "device ordinal out of range for static scratch");
+    std::lock_guard<std::mutex> lock(g_mb_mu);
+    if (!g_mb_ptr[dev]) {
+        unsigned char* ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_mb_scratch);
+        if (e != cudaSuccess || !ptr)
+            throw Error(MF3D_E_CUDA, std::string("cudaGetSymbolAddress(static scratch) failed: ") + cudaGetErrorString(e));
+        g_mb_ptr[dev] = ptr;
+    }
+    return g_mb_ptr[dev];
+}
+} // namespace
+
+int mf3d_velocity_mass_balance_noalloc(const mf3d_grid* g, const mf3d_bc* bc, const double* h, const double* K,
+                                       double* U, double* V, double* W, double* out_host, void* stream) {
+    return guard([&] {
+        check_grid(g);
+        need(bc, "bc");
+        validate_bc(*bc);
+        need(h, "h");
+        need(K, "K");
+        need(U, "U");
+        need(V, "V");
+        need(W, "W");
+        need(out_host, "out_host");
+        cudaStream_t s = (cudaStream_t)stream;
+        const ColLaunch cl = col_launch(g->nx, g->ny, g->nz);
+        if (cl.nblocks > kMbNoAllocMaxBlocks)
+            throw Error(MF3D_E_INVALID, "grid too large for the static mass-balance scratch: " + std::to_string(cl.nblocks) +
+                                            " reduction blocks needed, at most " +
+                                            std::to_string(kMbNoAllocMaxBlocks) +
+                                            " (ceil(nx/32) * ceil(ny/8) must not exceed it)");
+        unsigned char* base = mb_scratch_on_current_device();
+        unsigned long long* mx = (unsigned long long*)base;
+        unsigned* ticket = (unsigned*)(base + 8);
+        double* sums = (double*)(base + 16);
+        double* partials = (double*)(base + kMbNoAllocHeader);
+        // max bits, ticket and sums must start at zero; the partials are written before read
+        MF3D_CK(cudaMemsetAsync(base, 0, kMbNoAllocHeader, s));
+        VelOut o{U, V, W, MF3D_VEL_COMPACT};
+        velocity_kernel<<<cl.grid, cl.block, 0, s>>>(g->nx, g->ny, g->nz, g->dx, h, K, to_dev(*bc), o, mx, partials,
+                                                     ticket, sums, cl.zchunk);
+        MF3D_LAUNCH_CK();
+        unsigned long long hb[4];
+        MF3D_CK(cudaMemcpyAsync(hb, base, 32, cudaMemcpyDeviceToHost, s));
+        MF3D_CK(cudaStreamSynchronize(s));
+        std::memcpy(&out_host[0], &hb[0], 8);
+        std::memcpy(&out_host[1], &hb[2], 8);
+        std::memcpy(&out_host[2], &hb[3], 8);
     });
 }
 
