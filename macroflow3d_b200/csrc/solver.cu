@@ -192,15 +192,18 @@ template <class TC> static LevelOp<TC> make_op(const Geom& G, const mf3d_bc& bc,
 struct CoefStore {
     DevMem mem;
     template <class TC> void build(const Geom& G, size_t elt, LevelOp<TC>& L) {
-        const size_t pl = (size_t)G.ny * G.nz + (size_t)G.nx * G.nz + (size_t)G.nx * G.ny;
-        mem.alloc((3 * G.n + pl) * elt + 256);
+        // every array starts on a 256-byte boundary (TMA needs 16)
+        auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+        const size_t sc = up(G.n * elt), sbx = up((size_t)G.ny * G.nz * elt), sby = up((size_t)G.nx * G.nz * elt);
+        const size_t sbz = up((size_t)G.nx * G.ny * elt);
+        mem.alloc(3 * sc + sbx + sby + sbz);
         char* p = mem.as<char>();
         L.cx = (const TC*)p;
-        L.cy = (const TC*)(p + G.n * elt);
-        L.cz = (const TC*)(p + 2 * G.n * elt);
-        L.bxm = (const TC*)(p + 3 * G.n * elt);
-        L.bym = L.bxm + (size_t)G.ny * G.nz;
-        L.bzm = L.bym + (size_t)G.nx * G.nz;
+        L.cy = (const TC*)(p + sc);
+        L.cz = (const TC*)(p + 2 * sc);
+        L.bxm = (const TC*)(p + 3 * sc);
+        L.bym = (const TC*)(p + 3 * sc + sbx);
+        L.bzm = (const TC*)(p + 3 * sc + sbx + sby);
     }
 };
 
@@ -306,6 +309,22 @@ template <class E> static CUtensorMap make_map(const void* base, const Geom& g, 
     return m;
 }
 
+// 2-D tiled map over a d0*d1 array (the boundary-face planes), box b0*b1.
+template <class E> static CUtensorMap make_map2(const void* base, int d0, int d1, int b0, int b1) {
+    if (((uintptr_t)base & 15) || ((size_t)d0 * sizeof(E)) % 16)
+        throw Error(MF3D_E_INVALID, "array not aligned for TMA");
+    CUtensorMap m;
+    cuuint64_t dims[2] = {(cuuint64_t)d0, (cuuint64_t)d1};
+    cuuint64_t strides[1] = {(cuuint64_t)d0 * sizeof(E)};
+    cuuint32_t box[2] = {(cuuint32_t)b0, (cuuint32_t)b1};
+    cuuint32_t es[2] = {1u, 1u};
+    CUresult r = encode_fn()(&m, tma_dtype<E>(), 2, const_cast<void*>(base), dims, strides, box, es,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(MF3D_E_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return m;
+}
+
 template <class T, class TC> class VCycle : public VCycleBase {
   public:
     // b0: level-0 right-hand side in the V-cycle's type (the PCG residual or its FP32 copy);
@@ -353,7 +372,9 @@ template <class T, class TC> class VCycle : public VCycleBase {
                               bc.type[4] == MF3D_BC_PERIODIC;
         for (int l = 0; l < Lt && allow_tma && !periodic; ++l) {
             const Geom& g = G[l];
-            if ((g.nx * sizeof(T)) % 16 || (g.nx * sizeof(TC)) % 16 || g.nx < 16 || g.ny < 8) continue;
+            if ((g.nx * sizeof(T)) % 16 || (g.nx * sizeof(TC)) % 16 || (g.ny * sizeof(TC)) % 16 || g.nx < 16 ||
+                g.ny < 8)
+                continue;
             tma_[l] = 1;
             ++n_tma_;
             for (int resid = 0; resid < 2; ++resid) {
@@ -366,6 +387,9 @@ template <class T, class TC> class VCycle : public VCycleBase {
                 m.xa.cx = make_map<TC>(ops_[l].cx, g, bx, by);
                 m.xa.cy = make_map<TC>(ops_[l].cy, g, bx, by);
                 m.xa.cz = make_map<TC>(ops_[l].cz, g, bx, by);
+                m.xa.bxm = make_map2<TC>(ops_[l].bxm, g.ny, g.nz, TmaSweepCfg<T, TC, 0>::BYP, 1);
+                m.xa.bym = make_map2<TC>(ops_[l].bym, g.nx, g.nz, bx, 1);
+                m.xa.bzm = make_map2<TC>(ops_[l].bzm, g.nx, g.ny, bx, by);
                 m.xb = m.xa;
                 m.xb.x = make_map<T>(xb_[l]->p, g, bx, by);
             }
@@ -554,38 +578,21 @@ template <class T, class TC> class VCycle : public VCycleBase {
         return std::min(zc, ((g.nz + 1) & ~1));
     }
 
-    // z planes per CTA of the staged sweep: one CTA per SM, so pick the chunk count that
-    // minimises waves x (planes marched per CTA, halo planes included)
-    static int zchunk_tma(const Geom& g, long long nblk_xy, int halo) {
-        int best_zc = g.nz + (g.nz & 1);
-        double best = 1e300;
-        for (int nzc = 1; nzc <= std::min(g.nz, 64); ++nzc) {
-            int zc = (g.nz + nzc - 1) / nzc;
-            zc = (zc + 1) & ~1;
-            const int chunks = (g.nz + zc - 1) / zc;
-            const double waves = std::ceil((double)(nblk_xy * chunks) / num_sms());
-            const double cost = waves * (zc + 2 * halo);
-            if (cost < best - 1e-9) {
-                best = cost;
-                best_zc = zc;
-            }
-        }
-        return std::max(2, best_zc);
-    }
-
     void sweep(cudaStream_t s, int l, const T* x_in, T* x_out, const T* e, T* b_coarse, int mode, double* dot_out) {
         const Geom& g = G_[l];
         const bool tma = tma_[l] != 0;
         const int ty = tma ? tma_ty() : SW_TY;
         const int gx = (g.nx + SW_TX - 1) / SW_TX, gy = (g.ny + ty - 1) / ty;
-        const int zc = tma ? zchunk_tma(g, (long long)gx * gy, (mode & M_RESID) ? 3 : 2)
-                           : zchunk_for(g, gx * gy, num_sms() * 6);
-        const int gz = (g.nz + zc - 1) / zc;
-        dim3 grid(gx, gy, gz);
-        const unsigned nblk = (unsigned)gx * gy * gz;
-        if ((mode & M_DOT) && nblk > scr_.partial_cap) throw Error(MF3D_E_INVALID, "reduction scratch too small");
         const T* b = l == 0 ? b0_ : (const T*)bl_[l]->p;
         if (tma) {
+            // (tile, z chunk) CTAs, all resident at once: the most chunks per tile that fit
+            const long long ntiles = (long long)gx * gy;
+            const long long resident = (long long)std::max(1, occ_[mode & 15]) * num_sms();
+            const int nchunk = (int)std::max<long long>(1, std::min<long long>(g.nz / 2, resident / ntiles));
+            const int zc = 2 * (((g.nz + 1) / 2 + nchunk - 1) / nchunk);
+            const long long nblk = ntiles * ((g.nz + zc - 1) / zc);
+            const dim3 grid((unsigned)std::min(nblk, std::max(resident, ntiles)));
+            if ((mode & M_DOT) && grid.x > scr_.partial_cap) throw Error(MF3D_E_INVALID, "reduction scratch too small");
             TmaSweepArgs<T, TC> a{};
             a.L = ops_[l];
             a.x_out = x_out;
@@ -608,6 +615,11 @@ template <class T, class TC> class VCycle : public VCycleBase {
             dispatch_tma(s, grid, mode, maps, a);
             return;
         }
+        const int zc = zchunk_for(g, gx * gy, num_sms() * 6);
+        const int gz = (g.nz + zc - 1) / zc;
+        dim3 grid(gx, gy, gz);
+        const unsigned nblk = (unsigned)gx * gy * gz;
+        if ((mode & M_DOT) && nblk > scr_.partial_cap) throw Error(MF3D_E_INVALID, "reduction scratch too small");
         SweepArgs<T, TC, T> a{};
         a.L = ops_[l];
         a.b = b;
@@ -627,11 +639,16 @@ template <class T, class TC> class VCycle : public VCycleBase {
         dispatch(s, grid, mode, a);
     }
 
-    template <int MODE> static void set_one() {
+    template <int MODE> void set_one() {
+        using C = TmaSweepCfg<T, TC, MODE>;
         MF3D_CK(cudaFuncSetAttribute(sweep_tma_kernel<T, TC, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)TmaSweepCfg<T, TC, MODE>::SMEM));
+                                     (int)C::SMEM));
+        int n = 0;
+        MF3D_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_tma_kernel<T, TC, MODE>, C::NT, C::SMEM));
+        if (n < 1) throw Error(MF3D_E_CUDA, "staged sweep does not fit on an SM");
+        occ_[MODE & 15] = n;
     }
-    static void set_tma_smem() {
+    void set_tma_smem() {
         set_one<0>();
         set_one<M_ZERO>();
         set_one<M_PROLONG>();
@@ -713,6 +730,7 @@ template <class T, class TC> class VCycle : public VCycleBase {
     std::vector<int> tma_;
     std::vector<std::array<Maps4, 2>> maps_;
     int n_tma_ = 0;
+    int occ_[16] = {}; // resident staged-sweep CTAs per SM, by mode
     std::unique_ptr<DevMem> tail_out_, tail_w_;
     Tail2Args tail_{};
     size_t tail_smem_ = 0;
