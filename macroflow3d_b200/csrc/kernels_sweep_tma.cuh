@@ -9,29 +9,28 @@
 //   black cells of plane t-1 on the tile plus an RB = RR-1 ring,
 //   the residual of plane t-2 on the tile (RESID), restricted to the coarse right-hand side
 //   one step later, per pair of planes, and writes plane t-2 (now final) to global memory.
-// Every thread owns one pair of x-adjacent cells (one red, one black in every plane) in
-// every stage; the black cell of plane t-1 lies in the column of the red cell of plane t.
-// Every value a stage reads from another thread was written before the previous step's
-// barrier: ONE __syncthreads per plane.
+// Every thread owns one quad: four x-consecutive cells starting on a 16-byte boundary of the
+// staged box, two red and two black in every plane.  The black cells of plane t-1 lie in the
+// columns of the red cells of plane t.  All loads, the output and the residual move 16 bytes
+// per access.  Every value a stage reads from another thread was written before the previous
+// step's barrier: ONE __syncthreads per plane.
 //
-// Instruction economy.  The pairs of a warp all lie in rows of one parity, so the offset of
-// the red cell inside the pair, (row + t) & 1, is the same for the whole warp; the march is
-// unrolled by two and each step is compiled for its offset, with no per-cell selects.  The
-// stages compute unconditionally and predicate only their stores.  A pair's coefficients of
-// plane t are read from shared memory once; the black cell's ones are kept in registers for
-// the next step (double-buffered by the unrolling), and RESID keeps the whole pair for the
-// residual two steps later.  The -x and -y faces of the pair come from one precomputed
+// Instruction economy.  The quads of a warp all lie in rows of one parity, so the offset of
+// the red cells inside the quad, (row + t) & 1, is the same for the whole warp; the march is
+// unrolled by two and each step is compiled for its offset.  Stages compute unconditionally
+// and predicate only their stores.  Without RESID the black cells' coefficients of plane t
+// are kept in registers for the next step (double-buffered by the unrolling); RESID keeps
+// three coefficient planes staged instead and reads the black stage's and the residual's
+// coefficients from them.  The -x and -y faces of a quad come from one precomputed
 // shared-memory offset each, which points at the staged boundary faces on the min faces.
 //
 // Staging.  Two rings fed by cp.async.bulk.tensor.3d; thread 0 issues the copies and waits
 // on their mbarriers (bounded) at the end of the step before the one that reads them, so the
 // step barrier publishes the landed planes:
-//   x ring (NRX slots): planes t+1 .. t-2 are live at step t; plane t+1 is the red stage's
-//     upper z neighbour (corrected by the coarse correction in PROLONG mode), plane t holds
-//     the red updates, t-1 the black updates, t-2 the residual's reads and the output;
-//   coefficient ring (NRC slots): b, cx, cy, cz of plane t, plus the -x faces of the box rows
-//     and the -y faces of the box columns when the tile touches those boundaries; for plane -1
-//     the -z faces take the place of cz.
+//   x ring (NRX slots): planes t+1 .. t-2 are live at step t (box rows j0-H .. j0+TY+H-1);
+//   coefficient ring (NRC slots, LC live): b, cx, cz (rows j0-RR ..), cy (rows j0-H ..), the
+//     -x faces of the box rows and the -y faces of the box columns when the tile touches
+//     those boundaries; for plane -1 the -z faces take the place of cz.
 // Boxes start at x = i0 - HX with HX * sizeof(element) a multiple of 16 bytes (TMA's rule
 // for the innermost coordinate); y and z may start outside the grid, where TMA fills zeros:
 // the ghost value of a Dirichlet or Neumann face for x.  Periodic axes are served by
@@ -101,6 +100,20 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
     return false;
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Barrier `id` among the first `n` threads of the CTA, OR-reducing a flag.
+__device__ __forceinline__ bool bar_red_or(int id, int n, bool v) {
+    unsigned r;
+    asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, %3, p;\n selp.u32 %0, 1, 0, q;\n}"
+                 : "=r"(r)
+                 : "r"((unsigned)v), "r"(id), "r"(n)
+                 : "memory");
+    return r != 0;
+}
+
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int c0, int c1, uint64_t* bar) {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
@@ -124,22 +137,32 @@ template <class T, class TC, int MODE> struct TmaSweepCfg {
     static constexpr int RR = RESID ? 2 : 1; // red ring
     static constexpr int RB = RR - 1;        // black ring
     static constexpr int H = RR + 1;         // x halo read by the red ring
-    static constexpr int HX = TmaGeom<T, TC>::hx(H);
-    static constexpr int TX = 32, TY = sizeof(T) == 8 ? 8 : 16;
-    static constexpr int BX = TX + 2 * HX, BY = TY + 2 * H;
-    // pair items cover columns [i0-2, i0+TX+2) and rows [j0-RI, j0+TY+RI); PROLONG corrects
-    // the whole x halo, so its items reach ring H.  Half the warps take the even rows, half
-    // the odd ones.
-    static constexpr int RI = PROL ? H : RR;
-    static constexpr int IPW = TX / 2 + 2, IH = TY + 2 * RI;
-    static_assert(IH % 2 == 0, "rows come in parity pairs");
-    static constexpr int IPC = IPW * (IH / 2); // items per parity class
-    static constexpr int WPC = (IPC + 31) / 32;
-    static constexpr int NT = 2 * 32 * WPC;
-    static_assert(RI <= H && HX >= 2 && HX >= H, "pair items and their reads must stay inside the box");
+    static constexpr int TX = 64, TY = 8;
+    // quads start on 4-element boundaries of the box (16 bytes of T) and on TMA's alignment
+    static constexpr int HXA = TmaGeom<T, TC>::lcm_elts() > 4 ? TmaGeom<T, TC>::lcm_elts() : 4;
+    static constexpr int HX = ((4 + HXA - 1) / HXA) * HXA;
+    static constexpr int BX = TX + 2 * HX;
+    static constexpr int BY = TY + 2 * H;       // x box rows, from j0 - H
+    static constexpr int BYC = TY + 2 * RR;     // b, cx, cz box rows, from j0 - RR
+    static constexpr int BYY = TY + 2 * RR + 1; // cy box rows, from j0 - H
+    // quads cover columns [i0-4, i0+TX+4) and rows [j0-2, j0+TY+2) (ring 2 in every mode, so
+    // that the layout is the same; rows beyond the live ring compute nothing they store).
+    // The NMQ interior quads of a row lie in NMQ consecutive lanes; MW warps of interior
+    // quads per row parity, then one warp with the 2 edge quads of every row (both parities),
+    // then the producer warp.
+    static constexpr int NQ = TX / 4 + 2, NMQ = TX / 4, Q0 = HX - 4;
+    static constexpr int RI = 2;
+    static constexpr int IH = TY + 2 * RI, NRW = IH / 2;
+    static_assert(RR <= RI && (!PROL || H <= RI) && H <= 4, "quad rows cover the live rings inside the box");
+    static_assert((NMQ * NRW) % 32 == 0 && 4 * NRW <= 32, "interior quads fill whole warps, edge quads one");
+    static constexpr int MW = NMQ * NRW / 32;
+    static constexpr int NCONS = (2 * MW + 1) * 32; // consumer threads; one producer warp follows
+    static constexpr int NT = NCONS + 32;
     static constexpr size_t align128(size_t v) { return (v + 127) & ~(size_t)127; }
-    static constexpr size_t XB = (size_t)BX * BY * sizeof(T), CB = (size_t)BX * BY * sizeof(TC);
-    static constexpr size_t XS = align128(XB), CA = align128(CB);
+    static constexpr size_t XB = (size_t)BX * BY * sizeof(T);
+    static constexpr size_t BB = (size_t)BX * BYC * sizeof(T), CCB = (size_t)BX * BYC * sizeof(TC);
+    static constexpr size_t CYB = (size_t)BX * BYY * sizeof(TC);
+    static constexpr size_t XS = align128(XB);
     // -x boundary faces of the box rows, from row j0 - BYS (BYS * sizeof(TC) a multiple of 16)
     static constexpr int AL = 16 / (int)sizeof(TC);
     static constexpr int BYS = ((4 + AL - 1) / AL) * AL;
@@ -147,19 +170,23 @@ template <class T, class TC, int MODE> struct TmaSweepCfg {
     static_assert(BYS >= H, "boundary rows must cover the halo");
     static constexpr size_t BXMB = (size_t)BYP * sizeof(TC), BYMB = (size_t)BX * sizeof(TC);
     // coefficient slot: b, cx, cy, cz, bxm, bym
-    static constexpr size_t C_CX = XS, C_CY = XS + CA, C_CZ = XS + 2 * CA, C_BXM = XS + 3 * CA;
-    static constexpr size_t C_BYM = C_BXM + align128(BXMB);
+    static constexpr size_t C_CX = align128(BB), C_CY = C_CX + align128(CCB), C_CZ = C_CY + align128(CYB);
+    static constexpr size_t C_BXM = C_CZ + align128(CCB), C_BYM = C_BXM + align128(BXMB);
     static constexpr size_t CS = C_BYM + align128(BYMB);
+    static constexpr unsigned C_TX = (unsigned)(BB + 2 * CCB + CYB); // bytes of one plane without boundaries
     static constexpr size_t RS = RESID ? align128(3 * (size_t)TX * TY * sizeof(T)) : 0;
-    static constexpr int MINB = 2; // CTAs per SM
-    static constexpr size_t BUDGET = 110 * 1024;
+    // two CTAs per SM in FP32 (one CTA's barrier waits overlap the other's work); one in FP64
+    static constexpr int MINB = sizeof(T) == 8 ? 1 : 2;
+    static constexpr size_t BUDGET = MINB == 2 ? 112 * 1024 : 225 * 1024;
+    static constexpr int LC = RESID ? 3 : 1; // coefficient planes read at step t: t .. t-LC+1
+    // the x ring starts one guard row in: neighbour reads of edge quads may reach one box row
+    // before the first slot (they are never used)
+    static constexpr size_t GUARD = align128((size_t)BX * sizeof(T) + 16);
     static constexpr int NRX = 7; // 4 live x planes + 3 in flight
-    static constexpr int NRC_FIT = (int)((BUDGET - 256 - align128((size_t)BX * sizeof(T) + 16) - RS - NRX * XS) / CS);
+    static constexpr int NRC_FIT = (int)((BUDGET - 256 - GUARD - RS - NRX * XS) / CS);
     static constexpr int NRC = NRC_FIT < 8 ? NRC_FIT : 8;
-    static_assert(NRC >= 3, "coefficient ring too small");
-    // the x ring starts one guard row in: unpredicated neighbour reads of the edge items may
-    // reach one box row before the first slot (they are never used)
-    static constexpr size_t OFF_X = 256 + align128((size_t)BX * sizeof(T) + 16);
+    static_assert(NRC >= LC + 2 && 2 * (NRX + NRC) * 8 <= 256, "coefficient ring: two planes in flight");
+    static constexpr size_t OFF_X = 256 + GUARD;
     static constexpr size_t OFF_C = OFF_X + NRX * XS, OFF_R = OFF_C + NRC * CS;
     static constexpr size_t SMEM = OFF_R + RS;
 };
@@ -195,13 +222,44 @@ template <class T, class TC> __device__ __forceinline__ void lds_pair_as(const T
     }
 }
 
-// The black cell's coefficients of one plane, kept for the next step.
-template <class T> struct CellCoef {
-    T b, cxp, cxm, cyp, cym, czp;
+// Four consecutive values; lane k of a quad.
+template <class T> struct Q4 {
+    T v[4];
 };
-// A pair's coefficients of one plane (RESID keeps them for the residual).
-template <class T> struct PairCoef {
-    T b0, b1, cx0, cx1, cy0, cy1, cz0, cz1, cxl, cyd0, cyd1;
+template <class T, class E> __device__ __forceinline__ Q4<T> ldq(const E* p) {
+    Q4<T> q;
+    if constexpr (std::is_same<E, float>::value) {
+        const float4 a = *reinterpret_cast<const float4*>(p);
+        q.v[0] = (T)a.x, q.v[1] = (T)a.y, q.v[2] = (T)a.z, q.v[3] = (T)a.w;
+    } else if constexpr (std::is_same<E, double>::value) {
+        const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+        q.v[0] = (T)a.x, q.v[1] = (T)a.y, q.v[2] = (T)b.x, q.v[3] = (T)b.y;
+    } else {
+        const uint2 raw = *reinterpret_cast<const uint2*>(p);
+        const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.x));
+        const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.y));
+        q.v[0] = (T)a.x, q.v[1] = (T)a.y, q.v[2] = (T)b.x, q.v[3] = (T)b.y;
+    }
+    return q;
+}
+template <class T> __device__ __forceinline__ void stq(T* p, const Q4<T>& q) {
+    if constexpr (sizeof(T) == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4(q.v[0], q.v[1], q.v[2], q.v[3]);
+    } else {
+        reinterpret_cast<double2*>(p)[0] = make_double2(q.v[0], q.v[1]);
+        reinterpret_cast<double2*>(p)[1] = make_double2(q.v[2], q.v[3]);
+    }
+}
+// A quad's coefficients of one plane: b, the +x/+y/+z faces, the -y faces and the -x face
+// of cell 0 (the -x face of cell k > 0 is cx[k-1]).
+template <class T> struct QuadCoef {
+    Q4<T> b, cx, cy, cz, cyd;
+    T cxl;
+};
+// The two black cells' coefficients (cells O and O+2 of the next plane's quad), kept for the
+// next step.
+template <class T> struct BlackCoef {
+    T b[2], cxp[2], cxm[2], cyp[2], cym[2], czp[2];
 };
 
 template <class T, class TC, int MODE>
@@ -211,10 +269,16 @@ __global__ void __launch_bounds__(TmaSweepCfg<T, TC, MODE>::NT, TmaSweepCfg<T, T
     constexpr bool ZERO = C::ZERO, PROL = C::PROL, RESID = C::RESID;
     constexpr bool DOT = (MODE & M_DOT) != 0;
     constexpr int TX = C::TX, TY = C::TY, BX = C::BX, H = C::H, HX = C::HX, RR = C::RR, RB = C::RB;
-    constexpr int NRX = C::NRX, NRC = C::NRC;
+    constexpr int NRX = C::NRX, NRC = C::NRC, LC = C::LC;
     extern __shared__ __align__(128) unsigned char sweep_sm[];
+    // "full" barriers (a plane landed) of the x and coefficient rings, then "empty" barriers
+    // (the consumers released a slot)
     uint64_t* barx = reinterpret_cast<uint64_t*>(sweep_sm);
     uint64_t* barc = barx + NRX;
+    uint64_t* emx = barc + NRC;
+    uint64_t* emc = emx + NRX;
+    // planes issued so far by the producer (read by the consumers only to drain after a failure)
+    volatile int* issued = reinterpret_cast<volatile int*>(sweep_sm + 2 * 8 * (NRX + NRC));
     T* rsb = reinterpret_cast<T*>(sweep_sm + C::OFF_R);
     auto xsl = [&](int s) { return reinterpret_cast<T*>(sweep_sm + C::OFF_X + C::XS * s); };
     auto cbase = [&](int s) { return sweep_sm + C::OFF_C + C::CS * s; };
@@ -233,21 +297,26 @@ __global__ void __launch_bounds__(TmaSweepCfg<T, TC, MODE>::NT, TmaSweepCfg<T, T
     const int ntx = (nx + TX - 1) / TX, nty = (ny + TY - 1) / TY, ntiles = ntx * nty;
 
     if (tid == 0) {
-        for (int s = 0; s < NRX + NRC; ++s) mbar_init(&barx[s], 1);
+        for (int s = 0; s < 2 * (NRX + NRC); ++s) mbar_init(&barx[s], 1);
+        issued[0] = issued[1] = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
 
     // ring bookkeeping.  Every thread tracks the planes staged so far (qx, qc) and the slots of
-    // the planes it reads; thread 0 alone issues the copies and waits for them (phases in
-    // phx / phc).
+    // the planes it reads.  The producer warp's lane 0 issues the copies, each into a slot the
+    // consumers released; consumer thread 0 waits for the landed planes (phases in phx / phc)
+    // at the end of the step before the one that reads them, and releases the slots of the
+    // planes no longer read.
+    const bool producer = tid >= C::NCONS;
     unsigned qx = 0, qc = 0;
-    int xi_slot = 0, ci_slot = 0, xw_slot = 0, cw_slot = 0; // thread 0: next slot to issue / wait
+    int xw_slot = 0, cw_slot = 0, rx_slot = 0, rc_slot = 0; // consumer thread 0: next to wait / release
     unsigned phx = 0u, phc = 0u;
     double dot_acc = 0.0;
     bool fail = false;
     auto nxt_x = [](int s) { return s + 1 == NRX ? 0 : s + 1; };
     auto nxt_c = [](int s) { return s + 1 == NRC ? 0 : s + 1; };
+    auto prv_c = [](int s) { return s == 0 ? NRC - 1 : s - 1; };
     auto wait_x = [&]() { // thread 0
         const bool ok = mbar_wait(&barx[xw_slot], (phx >> xw_slot) & 1u);
         phx ^= 1u << xw_slot;
@@ -260,14 +329,42 @@ __global__ void __launch_bounds__(TmaSweepCfg<T, TC, MODE>::NT, TmaSweepCfg<T, T
         cw_slot = nxt_c(cw_slot);
         return ok;
     };
+    auto release_x = [&]() {
+        mbar_arrive(&emx[rx_slot]);
+        rx_slot = nxt_x(rx_slot);
+    };
+    auto release_c = [&]() {
+        mbar_arrive(&emc[rc_slot]);
+        rc_slot = nxt_c(rc_slot);
+    };
 
-    // ---- this thread's pair within a tile (tile-independent part) ----
-    const int cls = tid / (32 * C::WPC);        // row parity class of the warp
-    const int idx = tid - cls * (32 * C::WPC);  // item within the class
-    const bool iv = idx < C::IPC;
-    const int rr_ = iv ? idx / C::IPW : 0, ic = iv ? idx - rr_ * C::IPW : 1;
-    const int ir = 2 * rr_ + ((cls + C::RI) & 1); // item row, 0 .. IH-1; gj & 1 == cls
-    const int e = (ir - C::RI + H) * BX + (2 * ic - 2 + HX); // box element of the pair's left cell
+    // ---- this thread's quad within a tile (tile-independent part) ----
+    const int warp = tid >> 5, lane = tid & 31;
+    constexpr int NRW = C::NRW, NMQ = C::NMQ, MW = C::MW;
+    int cls = 0, rq = 0, qc_ = 1;
+    bool iv = false, mainq = false;
+    if (warp < 2 * MW) { // interior quads of one row parity
+        cls = warp / MW;
+        const int idx = (warp - cls * MW) * 32 + lane;
+        iv = mainq = true;
+        rq = idx / NMQ;
+        qc_ = 1 + idx % NMQ;
+    } else if (warp == 2 * MW && lane < 4 * NRW) { // edge quads: lanes by parity, then row
+        cls = lane >= 2 * NRW;
+        const int k = lane - cls * 2 * NRW;
+        iv = true;
+        rq = k >> 1;
+        qc_ = (k & 1) ? C::NQ - 1 : 0;
+    }
+    // the quads left and right of an interior quad are the neighbouring lanes, except at the
+    // ends of a row; the edge warp (both parities, diverging on the red offset) reads them
+    const bool fb_l = !(mainq && qc_ >= 2), fb_r = !(mainq && qc_ <= C::NQ - 3);
+    const bool edge_warp = warp >= 2 * MW; // uniform in a warp
+    auto from_left = [&](T v) { return edge_warp ? v : __shfl_up_sync(0xffffffffu, v, 1); };
+    auto from_right = [&](T v) { return edge_warp ? v : __shfl_down_sync(0xffffffffu, v, 1); };
+    const int ir = 2 * rq + ((cls + C::RI) & 1); // quad row, 0 .. IH-1; gj & 1 == cls
+    const int e = (ir - C::RI + H) * BX + C::Q0 + 4 * qc_;     // x (and cy) box element of cell 0
+    const int eC = e - (H - RR) * BX;                          // b, cx, cz box element of cell 0
 
     // CTA b: tile b % ntiles, z chunk b / ntiles (tiles fastest, so neighbouring tiles march
     // the same planes at the same time and share their halo rows in L2)
@@ -286,34 +383,58 @@ __global__ void __launch_bounds__(TmaSweepCfg<T, TC, MODE>::NT, TmaSweepCfg<T, T
         int t1 = RESID ? z1 + 2 : z1 + 1;
         if ((t1 - pl0 + 1) & 1) ++t1;
         const bool bnd_x = i0 == 0, bnd_y = j0 == 0;
-        int xi_plane = pl0, ci_plane = pl0; // thread 0: next plane to issue
+        if (producer) {
+            // ---- producer: both rings in order of need (x plane p is read one step before
+            // coefficient plane p), each copy into a slot the consumers have released ----
+            if (tid == C::NCONS) {
+                auto issue_x = [&](int p) {
+                    const unsigned n = qx + (unsigned)(p - pl0);
+                    const int s = (int)(n % NRX);
+                    if (n >= (unsigned)NRX && !mbar_wait(&emx[s], ((n / NRX) - 1) & 1u)) return false;
+                    mbar_expect_tx(&barx[s], (unsigned)C::XB);
+                    tma_load_3d(xsl(s), &maps.x, i0 - HX, j0 - H, p, &barx[s]);
+                    return true;
+                };
+                auto issue_c = [&](int p) {
+                    const unsigned n = qc + (unsigned)(p - pl0);
+                    const int s = (int)(n % NRC);
+                    if (n >= (unsigned)NRC && !mbar_wait(&emc[s], ((n / NRC) - 1) & 1u)) return false;
+                    uint64_t* bar = &barc[s];
+                    unsigned char* cs = cbase(s);
+                    mbar_expect_tx(bar, C::C_TX + (bnd_x ? (unsigned)C::BXMB : 0u) + (bnd_y ? (unsigned)C::BYMB : 0u));
+                    tma_load_3d(cs, &maps.b, i0 - HX, j0 - RR, p, bar);
+                    tma_load_3d(cs + C::C_CX, &maps.cx, i0 - HX, j0 - RR, p, bar);
+                    tma_load_3d(cs + C::C_CY, &maps.cy, i0 - HX, j0 - H, p, bar);
+                    if (p == -1) // the -z boundary faces stand in for plane -1's +z faces
+                        tma_load_2d(cs + C::C_CZ, &maps.bzm, i0 - HX, j0 - RR, bar);
+                    else
+                        tma_load_3d(cs + C::C_CZ, &maps.cz, i0 - HX, j0 - RR, p, bar);
+                    if (bnd_x) tma_load_2d(cs + C::C_BXM, &maps.bxm, j0 - C::BYS, p, bar);
+                    if (bnd_y) tma_load_2d(cs + C::C_BYM, &maps.bym, i0 - HX, p, bar);
+                    return true;
+                };
+                int px = ZERO ? xl1 + 1 : pl0, pc = pl0;
+                while (!fail && (px <= xl1 || pc <= cl1)) {
+                    if (px <= xl1 && (pc > cl1 || px <= pc + 1)) {
+                        fail = !issue_x(px);
+                        if (!fail) issued[0] = issued[0] + 1;
+                        ++px;
+                    } else {
+                        fail = !issue_c(pc);
+                        if (!fail) issued[1] = issued[1] + 1;
+                        ++pc;
+                    }
+                }
+                if (fail) atomicExch(a.err, 1);
+            }
+            if (!ZERO) qx += (unsigned)(xl1 - pl0 + 1);
+            qc += (unsigned)(cl1 - pl0 + 1);
+            continue;
+        }
+        // ---- consumers ----
         int xw_plane = pl0, cw_plane = pl0; // thread 0: next plane to wait for
-        auto issue_x = [&]() {
-            mbar_expect_tx(&barx[xi_slot], (unsigned)C::XB);
-            tma_load_3d(xsl(xi_slot), &maps.x, i0 - HX, j0 - H, xi_plane, &barx[xi_slot]);
-            xi_slot = nxt_x(xi_slot);
-            ++xi_plane;
-        };
-        auto issue_c = [&]() {
-            uint64_t* bar = &barc[ci_slot];
-            unsigned char* cs = cbase(ci_slot);
-            mbar_expect_tx(bar, (unsigned)(C::XB + 3 * C::CB + (bnd_x ? C::BXMB : 0) + (bnd_y ? C::BYMB : 0)));
-            tma_load_3d(cs, &maps.b, i0 - HX, j0 - H, ci_plane, bar);
-            tma_load_3d(cs + C::C_CX, &maps.cx, i0 - HX, j0 - H, ci_plane, bar);
-            tma_load_3d(cs + C::C_CY, &maps.cy, i0 - HX, j0 - H, ci_plane, bar);
-            if (ci_plane == -1) // the -z boundary faces stand in for plane -1's +z faces
-                tma_load_2d(cs + C::C_CZ, &maps.bzm, i0 - HX, j0 - H, bar);
-            else
-                tma_load_3d(cs + C::C_CZ, &maps.cz, i0 - HX, j0 - H, ci_plane, bar);
-            if (bnd_x) tma_load_2d(cs + C::C_BXM, &maps.bxm, j0 - C::BYS, ci_plane, bar);
-            if (bnd_y) tma_load_2d(cs + C::C_BYM, &maps.bym, i0 - HX, ci_plane, bar);
-            ci_slot = nxt_c(ci_slot);
-            ++ci_plane;
-        };
+        int xr_plane = pl0, cr_plane = pl0; // thread 0: next plane to release
         if (tid == 0) {
-            if (!ZERO)
-                while (xi_plane <= xl1 && xi_plane < pl0 + NRX) issue_x();
-            while (ci_plane <= cl1 && ci_plane < pl0 + NRC) issue_c();
             // the first step reads x planes pl0 and pl0 + 1 and coefficient plane pl0
             bool ok = true;
             if (!ZERO) {
@@ -330,201 +451,275 @@ __global__ void __launch_bounds__(TmaSweepCfg<T, TC, MODE>::NT, TmaSweepCfg<T, T
             }
             fail = !ok;
         }
-        fail = __syncthreads_or(fail) != 0;
-        // slots of x planes t+1, t, t-1, t-2 and of coefficient plane t (the same in every thread)
+        fail = bar_red_or(1, C::NCONS, fail);
+        // slots of x planes t+1, t, t-1, t-2 and of coefficient planes t, t-1, t-2 (the same in
+        // every thread)
         int sxp = nxt_x((int)(qx % NRX)), sx0 = (int)(qx % NRX), sx1 = 0, sx2 = 0;
-        int scc = (int)(qc % NRC);
+        int sc0 = (int)(qc % NRC);
 
-        // ---- the pair in this tile ----
-        const int gi = i0 - 2 + 2 * ic, gj = j0 - C::RI + ir;
-        const bool rowg = iv && gj >= 0 && gj < ny;
-        const bool g0 = rowg && gi >= 0 && gi < nx, g1 = rowg && gi + 1 >= 0 && gi + 1 < nx;
-        auto in_ring = [&](int i, int r) {
-            return iv && gj >= j0 - r && gj < j0 + TY + r && i >= i0 - r && i < i0 + TX + r;
-        };
-        const bool rr0 = in_ring(gi, RR), rr1 = in_ring(gi + 1, RR);
-        const bool rb0 = in_ring(gi, RB), rb1 = in_ring(gi + 1, RB);
-        const bool tl0 = in_ring(gi, 0) && g0, tl1 = in_ring(gi + 1, 0) && g1;
-        const bool pin_pair = L.pin && gi == 0 && gj == 0;
-        // byte offsets in a coefficient slot of the left cell's -x face and the pair's -y faces
+        // ---- the quad in this tile ----
+        const int gi = i0 - 4 + 4 * qc_, gj = j0 - C::RI + ir;
+        // per-cell flags, bit k for cell k: in grid (G), red ring (R), black ring (K), tile (T)
+        unsigned fg = 0u, fr = 0u, fk = 0u, ft = 0u;
+        {
+            const bool rowg = iv && gj >= 0 && gj < ny;
+            auto in_ring = [&](int i, int r) {
+                return iv && gj >= j0 - r && gj < j0 + TY + r && i >= i0 - r && i < i0 + TX + r;
+            };
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int i = gi + k;
+                const bool g = rowg && i >= 0 && i < nx;
+                fg |= (unsigned)g << k;
+                fr |= (unsigned)in_ring(i, RR) << k;
+                fk |= (unsigned)in_ring(i, RB) << k;
+                ft |= (unsigned)(g && in_ring(i, 0)) << k;
+            }
+        }
+        const bool pin_quad = L.pin && gi == 0 && gj == 0;
+        const bool tileq = (ft & 1u) != 0; // nx is a multiple of 4: a tile quad is all in or out
+        const bool restricts = RESID && tileq && ((gj - j0) & 1) == 0 && gj + 1 < ny;
+        // byte offsets in a coefficient slot of cell 0's -x face and the quad's -y faces
         const int off_cxl = (gi == 0) ? (int)C::C_BXM + (gj - (j0 - C::BYS)) * (int)sizeof(TC)
-                                      : (int)C::C_CX + (e - 1) * (int)sizeof(TC);
+                                      : (int)C::C_CX + (eC - 1) * (int)sizeof(TC);
         const int off_cyd = (gj == 0) ? (int)C::C_BYM + (gi - (i0 - HX)) * (int)sizeof(TC)
                                       : (int)C::C_CY + (e - BX) * (int)sizeof(TC);
         const int ncx = a.ncx;
         const size_t ncxy = (size_t)a.ncx * a.ncy;
-        const bool restricts = RESID && tl0 && ((gj - j0) & 1) == 0 && gj + 1 < ny;
-        // output item: VEC consecutive cells of one tile row (nx is a multiple of VEC)
-        constexpr int VEC = 16 / (int)sizeof(T), VPR = TX / VEC;
-        const int vr = tid / VPR, vc = tid - vr * VPR;
-        const bool vo_ok = tid < VPR * TY && j0 + vr < ny && i0 + VEC * vc < nx;
-        const int vo_e = (vr + H) * BX + HX + VEC * vc;
-        const size_t vo_g = (size_t)(i0 + VEC * vc) + (size_t)nx * (j0 + vr);
+        const size_t gq = (size_t)(gi > 0 ? gi : 0) + (size_t)nx * (gj > 0 ? gj : 0); // column of cell 0
 
-        // the pair's x_old in plane p (slot s) plus, in PROLONG mode, the coarse correction,
-        // stored back so that the neighbours read the corrected plane
-        auto own_x = [&](int p, int s, T& va, T& vb) {
-            va = (T)0;
-            vb = (T)0;
-            T* xs = xsl(s);
-            if (!ZERO) lds_pair<T>(xs + e, va, vb);
-            if (PROL) {
-                if (p >= 0 && p < nz && g0) { // nx is even: one coarse cell per pair
-                    const T ev = a.e_c[(size_t)(gi >> 1) + (size_t)ncx * (gj >> 1) + ncxy * (size_t)(p >> 1)];
-                    va += ev;
-                    vb += ev;
-                }
-                if (iv) st_pair<T>(xs + e, va, vb);
+        auto load_coef = [&](int s) {
+            const unsigned char* cs = cbase(s);
+            QuadCoef<T> c;
+            c.b = ldq<T>(reinterpret_cast<const T*>(cs) + eC);
+            c.cx = ldq<T>(reinterpret_cast<const TC*>(cs + C::C_CX) + eC);
+            c.cy = ldq<T>(reinterpret_cast<const TC*>(cs + C::C_CY) + e);
+            c.cz = ldq<T>(reinterpret_cast<const TC*>(cs + C::C_CZ) + eC);
+            c.cyd = ldq<T>(reinterpret_cast<const TC*>(cs + off_cyd));
+            c.cxl = from_left(c.cx.v[3]); // the left quad's last +x face
+            if (fb_l || gi == 0) c.cxl = tc(*reinterpret_cast<const TC*>(cs + off_cxl));
+            return c;
+        };
+        auto cz_of = [&](int s) { return ldq<T>(reinterpret_cast<const TC*>(cbase(s) + C::C_CZ) + eC); };
+        // coarse correction of the quad in plane p (cells 0-1 and 2-3 share coarse cells)
+        auto load_ev = [&](int p, T& e0, T& e1) {
+            e0 = e1 = (T)0;
+            if (!PROL || !(p >= 0 && p < nz && (fg & 1u))) return;
+            const T* src = a.e_c + (size_t)(gi >> 1) + (size_t)ncx * (gj >> 1) + ncxy * (size_t)(p >> 1);
+            e0 = src[0];
+            if (fg & 4u) e1 = src[1];
+        };
+        auto restrict_quad = [&](int s1, int rs0, int rs1) { // coarse plane s1 >> 1 from s1 - 1, s1
+            const T* r0 = rsb + rs0 * TX * TY + (gj - j0) * TX + (gi - i0);
+            const T* r1 = rsb + rs1 * TX * TY + (gj - j0) * TX + (gi - i0);
+            const Q4<T> a0 = ldq<T>(r0), a1 = ldq<T>(r0 + TX), b0 = ldq<T>(r1), b1 = ldq<T>(r1 + TX);
+            T o[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                T acc = (T)0;
+                acc += a0.v[2 * h];
+                acc += a0.v[2 * h + 1];
+                acc += a1.v[2 * h];
+                acc += a1.v[2 * h + 1];
+                acc += b0.v[2 * h];
+                acc += b0.v[2 * h + 1];
+                acc += b1.v[2 * h];
+                acc += b1.v[2 * h + 1];
+                o[h] = acc / (T)8;
             }
-        };
-        auto restrict_pair = [&](int s1, int rs0, int rs1) { // coarse plane s1 >> 1 from s1 - 1, s1
-            const T* r0 = rsb + rs0 * TX * TY;
-            const T* r1 = rsb + rs1 * TX * TY;
-            const int f = (gj - j0) * TX + (gi - i0);
-            T acc = (T)0;
-            acc += r0[f];
-            acc += r0[f + 1];
-            acc += r0[f + TX];
-            acc += r0[f + TX + 1];
-            acc += r1[f];
-            acc += r1[f + 1];
-            acc += r1[f + TX];
-            acc += r1[f + TX + 1];
-            a.b_coarse[(size_t)(gi >> 1) + (size_t)ncx * (gj >> 1) + ncxy * (size_t)(s1 >> 1)] = acc / (T)8;
+            T* dst = a.b_coarse + (size_t)(gi >> 1) + (size_t)ncx * (gj >> 1) + ncxy * (size_t)(s1 >> 1);
+            dst[0] = o[0];
+            dst[1] = o[1];
         };
 
-        // carried state: the black cell's coefficients of the previous plane (cbA / cbB), the
-        // red cell's +z face of two planes back (czA / czB), and in RESID the whole pair of
-        // planes t-1, t-2 (c1, c2), cz of plane t-3 and the pair's final x of plane t-3
-        CellCoef<T> cbA{}, cbB{};
-        T czA = 0, czB = 0;
-        PairCoef<T> c1{}, c2{};
-        T cz3a = 0, cz3b = 0, x3a = 0, x3b = 0;
-        int rslot = 0; // rsb slot of residual plane t-2 ((t - 2 - z0) mod 3)
+        // carried state (non-RESID): the black cells' coefficients of the previous plane and the
+        // red cells' +z faces of two planes back; RESID: cz of plane t-3 and the final x of t-3
+        BlackCoef<T> cbA{}, cbB{};
+        T czA[2] = {0, 0}, czB[2] = {0, 0};
+        Q4<T> cz3{}, x3{};
+        T evA0 = 0, evA1 = 0; // PROLONG: correction of plane t+2, loaded one step ahead
+        int rslot = 0;        // rsb slot of residual plane t-2 ((t - 2 - z0) mod 3)
 
-        // one step of the march; O: offset of the red cell of plane t in the pair (compile time)
-        auto step = [&](auto Oc, int t, CellCoef<T>& cb_in, CellCoef<T>& cb_out, T& cz_io) {
+        // one step of the march; O: offset of the first red cell of plane t in the quad
+        auto step = [&](auto Oc, int t, BlackCoef<T>& cb_in, BlackCoef<T>& cb_out, T (&cz_io)[2]) {
             constexpr int O = decltype(Oc)::value;
-            // -------- refill the slots freed by the previous step (thread 0) --------
-            if (tid == 0) {
-                if (!ZERO && t - 3 >= pl0 && xi_plane <= xl1) issue_x();
-                if (t - 1 >= pl0 && ci_plane <= cl1) issue_c();
-            }
             const bool in_z = t >= 0 && t < nz;
-            // -------- the pair's x in plane t+1 (and t at the start), corrected --------
-            T xpa = 0, xpb = 0;
-            if (t == pl0) {
-                T d0, d1;
-                own_x(t, sx0, d0, d1);
-            }
-            if (t + 1 <= xl1) own_x(t + 1, sxp, xpa, xpb);
-            // -------- coefficients of plane t --------
-            PairCoef<T> c0;
-            {
-                const unsigned char* cs = cbase(scc);
-                lds_pair<T>(reinterpret_cast<const T*>(cs) + e, c0.b0, c0.b1);
-                lds_pair_as<T, TC>(reinterpret_cast<const TC*>(cs + C::C_CX) + e, c0.cx0, c0.cx1);
-                lds_pair_as<T, TC>(reinterpret_cast<const TC*>(cs + C::C_CY) + e, c0.cy0, c0.cy1);
-                lds_pair_as<T, TC>(reinterpret_cast<const TC*>(cs + C::C_CZ) + e, c0.cz0, c0.cz1);
-                lds_pair_as<T, TC>(reinterpret_cast<const TC*>(cs + off_cyd), c0.cyd0, c0.cyd1);
-                c0.cxl = tc(*reinterpret_cast<const TC*>(cs + off_cxl));
-            }
-            // -------- red, plane t, cell O --------
-            T vred;
-            {
-                const T cxp = O ? c0.cx1 : c0.cx0, cxm = O ? c0.cx0 : c0.cxl;
-                const T cyp = O ? c0.cy1 : c0.cy0, cym = O ? c0.cyd1 : c0.cyd0;
-                const T czp = O ? c0.cz1 : c0.cz0, czm = cb_in.czp; // cz(t-1) of this cell
-                T D = cxm + cxp + cym + cyp + czm + czp;
-                if (pin_pair && O == 0 && t == 0) D *= (T)2;
-                T s = (T)0;
-                T* xs = xsl(sx0);
-                if (!ZERO) {
-                    const T xr = xs[e + O + 1], xl = xs[e + O - 1];
-                    s = cxp * xr + cxm * xl + cyp * xs[e + O + BX] + cym * xs[e + O - BX] + czp * (O ? xpb : xpa) +
-                        czm * xsl(sx1)[e + O];
+            const int q = t - 1, sp = t - 2;
+            T* xs0 = xsl(sx0);
+            T* xs1 = xsl(sx1);
+            T* xs2 = xsl(sx2);
+            const int sc1 = prv_c(sc0), sc2 = prv_c(sc1);
+            // ======== loads of the red and black stages ========
+            Q4<T> xp{};
+            T ev0, ev1;
+            if (t == pl0) { // the first plane: its x_old, corrected
+                T f0, f1;
+                load_ev(t, f0, f1);
+                if (PROL && iv) {
+                    Q4<T> v = ZERO ? Q4<T>{} : ldq<T>(xs0 + e);
+                    v.v[0] += f0, v.v[1] += f0, v.v[2] += f1, v.v[3] += f1;
+                    stq<T>(xs0 + e, v);
                 }
-                const bool live = t >= t0 && t <= cl1 && (O ? rr1 : rr0);
-                vred = (in_z && (O ? g1 : g0)) ? divide(s - (O ? c0.b1 : c0.b0) * dx2, D) : (T)0;
-                if (live) xs[e + O] = vred;
-                // the black cell of plane t (the other one) is updated at the next step
-                if (O == 0) cb_out = CellCoef<T>{c0.b1, c0.cx1, c0.cx0, c0.cy1, c0.cyd1, c0.cz1};
-                else cb_out = CellCoef<T>{c0.b0, c0.cx0, c0.cxl, c0.cy0, c0.cyd0, c0.cz0};
+                load_ev(t + 1, ev0, ev1);
+            } else {
+                ev0 = evA0, ev1 = evA1;
             }
-            // -------- black, plane t-1, cell O --------
-            {
-                const int q = t - 1;
-                const T czm = cz_io; // cz(t-2) of this cell: the red cell's +z face two steps back
-                const T D = cb_in.cxm + cb_in.cxp + cb_in.cym + cb_in.cyp + czm + cb_in.czp;
-                T* xs = xsl(sx1);
-                const T xr = xs[e + O + 1], xl = xs[e + O - 1];
-                const T s = cb_in.cxp * xr + cb_in.cxm * xl + cb_in.cyp * xs[e + O + BX] + cb_in.cym * xs[e + O - BX] +
-                            cb_in.czp * vred + czm * xsl(sx2)[e + O];
-                const bool live = q >= z0 - RB && q < z1 + RB && (O ? rb1 : rb0);
-                const T v = (q >= 0 && q < nz && (O ? g1 : g0)) ? divide(s - cb_in.b * dx2, D) : (T)0;
-                if (live) xs[e + O] = v;
+            if (PROL) load_ev(t + 2, evA0, evA1);
+            if (t + 1 <= xl1) {
+                if (!ZERO) xp = ldq<T>(xsl(sxp) + e);
+                xp.v[0] += ev0, xp.v[1] += ev0, xp.v[2] += ev1, xp.v[3] += ev1;
             }
-            cz_io = O ? c0.cz1 : c0.cz0; // for the black stage two steps on
-            // -------- plane t-2 is final: write the tile, 16 bytes per thread --------
-            if (t - 2 >= z0 && t - 2 < z1 && vo_ok) {
-                const T* xs = xsl(sx2);
-                const size_t cg = vo_g + nxy * (size_t)(t - 2);
-                if constexpr (sizeof(T) == 4) {
-                    const float4 v = *reinterpret_cast<const float4*>(xs + vo_e);
-                    *reinterpret_cast<float4*>(a.x_out + cg) = v;
-                    if (DOT) {
-                        const double2 r0 = __ldg(reinterpret_cast<const double2*>(a.r64 + cg));
-                        const double2 r1 = __ldg(reinterpret_cast<const double2*>(a.r64 + cg + 2));
-                        dot_acc += r0.x * (double)v.x + r0.y * (double)v.y + r1.x * (double)v.z + r1.y * (double)v.w;
-                    }
-                } else {
-                    const double2 v = *reinterpret_cast<const double2*>(xs + vo_e);
-                    *reinterpret_cast<double2*>(a.x_out + cg) = v;
-                    if (DOT) {
-                        const double2 r0 = __ldg(reinterpret_cast<const double2*>(a.r64 + cg));
-                        dot_acc += r0.x * (double)v.x + r0.y * (double)v.y;
-                    }
+            const QuadCoef<T> c0 = load_coef(sc0);
+            Q4<T> x0{}, x0u{}, x0d{};
+            T x0o = 0;
+            if (!ZERO) {
+                x0 = ldq<T>(xs0 + e);
+                x0u = ldq<T>(xs0 + e + BX);
+                x0d = ldq<T>(xs0 + e - BX);
+                x0o = O ? from_right(x0.v[0]) : from_left(x0.v[3]);
+                if (O ? fb_r : fb_l) x0o = O ? xs0[e + 4] : xs0[e - 1];
+            }
+            const Q4<T> x1 = ldq<T>(xs1 + e), x1u = ldq<T>(xs1 + e + BX), x1d = ldq<T>(xs1 + e - BX);
+            T x1o = O ? from_right(x1.v[0]) : from_left(x1.v[3]);
+            if (O ? fb_r : fb_l) x1o = O ? xs1[e + 4] : xs1[e - 1];
+            const Q4<T> x2 = ldq<T>(xs2 + e);
+            // coefficients of the black cells (plane t-1) and the +z faces of planes t-1, t-2
+            T bb[2], bxp[2], bxm[2], byp[2], bym_[2], bzp[2], bzm_[2], rzm[2];
+            if constexpr (RESID) {
+                const QuadCoef<T> c1 = load_coef(sc1);
+                const Q4<T> z2 = cz_of(sc2);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int k = O + 2 * h;
+                    bb[h] = c1.b.v[k];
+                    bxp[h] = c1.cx.v[k];
+                    bxm[h] = k == 0 ? c1.cxl : c1.cx.v[k - 1];
+                    byp[h] = c1.cy.v[k];
+                    bym_[h] = c1.cyd.v[k];
+                    bzp[h] = c1.cz.v[k];
+                    bzm_[h] = z2.v[k];
+                    rzm[h] = c1.cz.v[k];
                 }
+            } else {
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    bb[h] = cb_in.b[h];
+                    bxp[h] = cb_in.cxp[h];
+                    bxm[h] = cb_in.cxm[h];
+                    byp[h] = cb_in.cyp[h];
+                    bym_[h] = cb_in.cym[h];
+                    bzp[h] = cb_in.czp[h];
+                    bzm_[h] = cz_io[h];
+                    rzm[h] = cb_in.czp[h];
+                }
+            }
+            double2 r64a = make_double2(0.0, 0.0), r64b = make_double2(0.0, 0.0);
+            const bool out_t = sp >= z0 && sp < z1 && tileq;
+            const size_t cg_out = gq + nxy * (size_t)(sp > 0 ? sp : 0);
+            if (DOT && out_t) {
+                r64a = __ldg(reinterpret_cast<const double2*>(a.r64 + cg_out));
+                r64b = __ldg(reinterpret_cast<const double2*>(a.r64 + cg_out + 2));
+            }
+            // ======== arithmetic ========
+            T vred[2], vblk[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int k = O + 2 * h; // cell of the quad
+                // red, plane t
+                {
+                    const T cxp = c0.cx.v[k], cxm = k == 0 ? c0.cxl : c0.cx.v[k - 1];
+                    const T cyp = c0.cy.v[k], cym = c0.cyd.v[k], czp = c0.cz.v[k], czm = rzm[h];
+                    T D = cxm + cxp + cym + cyp + czm + czp;
+                    if (k == 0 && t == 0 && pin_quad) D *= (T)2;
+                    T s = (T)0;
+                    if (!ZERO) {
+                        const T xl = k == 0 ? x0o : x0.v[k - 1], xr = k == 3 ? x0o : x0.v[k + 1];
+                        s = cxp * xr + cxm * xl + cyp * x0u.v[k] + cym * x0d.v[k] + czp * xp.v[k] + czm * x1.v[k];
+                    }
+                    vred[h] = (in_z && ((fg >> k) & 1u)) ? divide(s - c0.b.v[k] * dx2, D) : (T)0;
+                }
+                // black, plane t-1
+                {
+                    const T D = bxm[h] + bxp[h] + bym_[h] + byp[h] + bzm_[h] + bzp[h];
+                    const T xl = k == 0 ? x1o : x1.v[k - 1], xr = k == 3 ? x1o : x1.v[k + 1];
+                    const T s = bxp[h] * xr + bxm[h] * xl + byp[h] * x1u.v[k] + bym_[h] * x1d.v[k] + bzp[h] * vred[h] +
+                                bzm_[h] * x2.v[k];
+                    vblk[h] = (q >= 0 && q < nz && ((fg >> k) & 1u)) ? divide(s - bb[h] * dx2, D) : (T)0;
+                }
+            }
+            if constexpr (!RESID) {
+                // the black cells of plane t (cells 1-O, 3-O) are updated at the next step
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int k = (1 - O) + 2 * h;
+                    cb_out.b[h] = c0.b.v[k];
+                    cb_out.cxp[h] = c0.cx.v[k];
+                    cb_out.cxm[h] = k == 0 ? c0.cxl : c0.cx.v[k - 1];
+                    cb_out.cyp[h] = c0.cy.v[k];
+                    cb_out.cym[h] = c0.cyd.v[k];
+                    cb_out.czp[h] = c0.cz.v[k];
+                    cz_io[h] = c0.cz.v[O + 2 * h]; // for the black stage two steps on
+                }
+            }
+            // ======== stores of the red and black stages ========
+            const bool red_live = t >= t0 && t <= cl1, blk_live = q >= z0 - RB && q < z1 + RB;
+            // whole quads: the cells not updated are written back with the values just read
+            // (zero in ZERO mode, where nothing reads them before they are updated)
+            constexpr unsigned OM = (1u << O) | (4u << O);
+            if (red_live && (fr & OM)) {
+                Q4<T> w = x0;
+                if ((fr >> O) & 1u) w.v[O] = vred[0];
+                if ((fr >> (O + 2)) & 1u) w.v[O + 2] = vred[1];
+                stq<T>(xs0 + e, w);
+            }
+            if (blk_live && (fk & OM)) {
+                Q4<T> w = x1;
+                if ((fk >> O) & 1u) w.v[O] = vblk[0];
+                if ((fk >> (O + 2)) & 1u) w.v[O + 2] = vblk[1];
+                stq<T>(xs1 + e, w);
+            }
+            if (PROL && iv && t + 1 <= xl1) stq<T>(xsl(sxp) + e, xp);
+            // -------- plane t-2 is final: write the tile --------
+            if (out_t) {
+                stq<T>(a.x_out + cg_out, x2);
+                if constexpr (DOT)
+                    dot_acc += r64a.x * (double)x2.v[0] + r64a.y * (double)x2.v[1] + r64b.x * (double)x2.v[2] +
+                               r64b.y * (double)x2.v[3];
             }
             if constexpr (RESID) {
                 // -------- residual, plane t-2 (smoother's pin convention) --------
-                const int sp = t - 2;
-                const T* xs = xsl(sx2);
-                T x2a, x2b, x1a, x1b, ua, ub, da, db;
-                lds_pair<T>(xs + e, x2a, x2b);
-                lds_pair<T>(xsl(sx1) + e, x1a, x1b);
-                lds_pair<T>(xs + e + BX, ua, ub);
-                lds_pair<T>(xs + e - BX, da, db);
-                const T xl = xs[e - 1], xr = xs[e + 2];
-                T ra, rb;
-                {
-                    const T cxp = c2.cx0, cxm = c2.cxl, cyp = c2.cy0, cym = c2.cyd0, czp = c2.cz0, czm = cz3a;
+                const QuadCoef<T> c2 = load_coef(sc2);
+                const Q4<T> x2u = ldq<T>(xs2 + e + BX), x2d = ldq<T>(xs2 + e - BX);
+                T x2l = from_left(x2.v[3]), x2r = from_right(x2.v[0]);
+                if (fb_l) x2l = xs2[e - 1];
+                if (fb_r) x2r = xs2[e + 4];
+                Q4<T> x1f = x1; // final x of plane t-1
+                x1f.v[O] = vblk[0];
+                x1f.v[O + 2] = vblk[1];
+                Q4<T> r;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const T cxp = c2.cx.v[k], cxm = k == 0 ? c2.cxl : c2.cx.v[k - 1];
+                    const T cyp = c2.cy.v[k], cym = c2.cyd.v[k], czp = c2.cz.v[k], czm = cz3.v[k];
                     T D = cxm + cxp + cym + cyp + czm + czp;
-                    if (pin_pair && sp == 0) D *= (T)2;
-                    const T sum = cxp * x2b + cxm * xl + cyp * ua + cym * da + czp * x1a + czm * x3a;
-                    ra = c2.b0 - (sum - D * x2a) * inv_dx2;
+                    if (k == 0 && sp == 0 && pin_quad) D *= (T)2;
+                    const T xl = k == 0 ? x2l : x2.v[k - 1], xr = k == 3 ? x2r : x2.v[k + 1];
+                    const T sum = cxp * xr + cxm * xl + cyp * x2u.v[k] + cym * x2d.v[k] + czp * x1f.v[k] + czm * x3.v[k];
+                    r.v[k] = c2.b.v[k] - (sum - D * x2.v[k]) * inv_dx2;
                 }
-                {
-                    const T cxp = c2.cx1, cxm = c2.cx0, cyp = c2.cy1, cym = c2.cyd1, czp = c2.cz1, czm = cz3b;
-                    const T D = cxm + cxp + cym + cyp + czm + czp;
-                    const T sum = cxp * xr + cxm * x2a + cyp * ub + cym * db + czp * x1b + czm * x3b;
-                    rb = c2.b1 - (sum - D * x2b) * inv_dx2;
-                }
-                if (sp >= z0 && sp < z1 && (tl0 || tl1))
-                    st_pair<T>(rsb + rslot * TX * TY + (gj - j0) * TX + (gi - i0), tl0 ? ra : (T)0, tl1 ? rb : (T)0);
+                if (sp >= z0 && sp < z1 && tileq) stq<T>(rsb + rslot * TX * TY + (gj - j0) * TX + (gi - i0), r);
                 // -------- restriction of planes (t-4, t-3), finished before the last barrier --------
                 const int s1 = t - 3;
                 if (restricts && s1 > z0 && s1 < z1 && ((s1 - z0) & 1) == 1)
-                    restrict_pair(s1, rslot == 0 ? 1 : rslot - 1 == 0 ? 2 : rslot - 2, rslot == 0 ? 2 : rslot - 1);
+                    restrict_quad(s1, rslot == 0 ? 1 : rslot - 1 == 0 ? 2 : rslot - 2, rslot == 0 ? 2 : rslot - 1);
                 if (sp >= z0) rslot = rslot == 2 ? 0 : rslot + 1;
-                x3a = x2a;
-                x3b = x2b;
-                cz3a = c2.cz0;
-                cz3b = c2.cz1;
-                c2 = c1;
-                c1 = c0;
+                x3 = x2;
+                cz3 = c2.cz;
             }
-            // -------- thread 0: wait for the planes of the next step --------
+        };
+        // the end of a step, common to both offsets: thread 0 waits for the planes of the next
+        // step; the barrier publishes them and the plane exchange; the next step's slots
+        auto sync_step = [&](int t) {
             if (tid == 0 && t < t1) {
                 bool ok = true;
                 if (!ZERO && xw_plane <= xl1) {
@@ -540,44 +735,65 @@ __global__ void __launch_bounds__(TmaSweepCfg<T, TC, MODE>::NT, TmaSweepCfg<T, T
             // generic-proxy writes to the rings are ordered before the TMA writes that reuse
             // the slots; the barrier completes the hand-off and the plane exchange
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            fail = __syncthreads_or(fail) != 0;
+            fail = bar_red_or(1, C::NCONS, fail);
             sx2 = sx1;
             sx1 = sx0;
             sx0 = sxp;
             sxp = nxt_x(sxp);
-            scc = nxt_c(scc);
+            sc0 = nxt_c(sc0);
+        };
+
+        // the start of a step: thread 0 releases the slots no longer read
+        auto release_step = [&](int t) {
+            if (tid == 0) {
+                if (!ZERO && t - 3 >= pl0 && xr_plane <= xl1) {
+                    release_x();
+                    ++xr_plane;
+                }
+                if (t - LC >= pl0 && cr_plane <= cl1) {
+                    release_c();
+                    ++cr_plane;
+                }
+            }
         };
 
         using Z = std::integral_constant<int, 0>;
         using I = std::integral_constant<int, 1>;
         for (int t = pl0; t < t1 && !fail; t += 2) {
-            // red offset of plane t: (gj + t) & 1 = (cls + t) & 1, uniform in the warp
-            if (((cls + t) & 1) == 0) step(Z{}, t, cbB, cbA, czA);
+            // red offset of plane t: (gj + t) & 1 = (cls + t) & 1, uniform in a warp of interior
+            // quads; the edge warp holds both parities and runs both offsets in turn
+            const bool even = ((cls + t) & 1) == 0;
+            release_step(t);
+            if (even) step(Z{}, t, cbB, cbA, czA);
             else step(I{}, t, cbB, cbA, czA);
+            sync_step(t);
             if (fail) break;
-            if (((cls + t) & 1) == 0) step(I{}, t + 1, cbA, cbB, czB);
+            release_step(t + 1);
+            if (even) step(I{}, t + 1, cbA, cbB, czB);
             else step(Z{}, t + 1, cbA, cbB, czB);
+            sync_step(t + 1);
         }
         if (fail) {
-            // drain this CTA's copies in flight (bounded waits), then leave
+            // drain the copies issued and not yet waited for (bounded waits), then leave
             if (tid == 0) {
                 atomicExch(a.err, 1);
-                while (xw_plane < xi_plane) {
-                    (void)wait_x();
-                    ++xw_plane;
-                }
-                while (cw_plane < ci_plane) {
-                    (void)wait_c();
-                    ++cw_plane;
-                }
+                const int nx_done = (int)qx + (xw_plane - pl0), nc_done = (int)qc + (cw_plane - pl0);
+                for (int k = nx_done; k < issued[0]; ++k) (void)wait_x();
+                for (int k = nc_done; k < issued[1]; ++k) (void)wait_c();
             }
             break;
+        }
+        // release the planes still held, so that the producer can reuse their slots
+        if (tid == 0) {
+            if (!ZERO)
+                for (; xr_plane <= xl1; ++xr_plane) release_x();
+            for (; cr_plane <= cl1; ++cr_plane) release_c();
         }
         if (!ZERO) qx += (unsigned)(xl1 - pl0 + 1);
         qc += (unsigned)(cl1 - pl0 + 1);
     }
 
-    if (DOT && !fail) {
+    if (DOT) { // every thread, the producer warp included (grid_sums synchronises the CTA)
         double v[1] = {dot_acc}, out[1];
         if (grid_sums<C::NT, 1>(v, a.dot_partials, a.dot_ticket, gridDim.x, out)) *a.dot_out = out[0];
     }

@@ -378,18 +378,21 @@ template <class T, class TC> class VCycle : public VCycleBase {
             tma_[l] = 1;
             ++n_tma_;
             for (int resid = 0; resid < 2; ++resid) {
-                const int H = resid ? 3 : 2;
-                const int bx = SW_TX + 2 * TmaGeom<T, TC>::hx(H), by = tma_ty() + 2 * H;
+                // box shapes of the staged sweep: x (BX x BY), b / cx / cz (BX x BYC), cy (BX x BYY)
+                const int bx = resid ? TmaSweepCfg<T, TC, M_RESID>::BX : TmaSweepCfg<T, TC, 0>::BX;
+                const int by = resid ? TmaSweepCfg<T, TC, M_RESID>::BY : TmaSweepCfg<T, TC, 0>::BY;
+                const int byc = resid ? TmaSweepCfg<T, TC, M_RESID>::BYC : TmaSweepCfg<T, TC, 0>::BYC;
+                const int byy = resid ? TmaSweepCfg<T, TC, M_RESID>::BYY : TmaSweepCfg<T, TC, 0>::BYY;
                 Maps4& m = maps_[l][resid];
                 const T* b = l == 0 ? b0_ : (const T*)bl_[l]->p;
                 m.xa.x = make_map<T>(xa_[l]->p, g, bx, by);
-                m.xa.b = make_map<T>(b, g, bx, by);
-                m.xa.cx = make_map<TC>(ops_[l].cx, g, bx, by);
-                m.xa.cy = make_map<TC>(ops_[l].cy, g, bx, by);
-                m.xa.cz = make_map<TC>(ops_[l].cz, g, bx, by);
+                m.xa.b = make_map<T>(b, g, bx, byc);
+                m.xa.cx = make_map<TC>(ops_[l].cx, g, bx, byc);
+                m.xa.cy = make_map<TC>(ops_[l].cy, g, bx, byy);
+                m.xa.cz = make_map<TC>(ops_[l].cz, g, bx, byc);
                 m.xa.bxm = make_map2<TC>(ops_[l].bxm, g.ny, g.nz, TmaSweepCfg<T, TC, 0>::BYP, 1);
                 m.xa.bym = make_map2<TC>(ops_[l].bym, g.nx, g.nz, bx, 1);
-                m.xa.bzm = make_map2<TC>(ops_[l].bzm, g.nx, g.ny, bx, by);
+                m.xa.bzm = make_map2<TC>(ops_[l].bzm, g.nx, g.ny, bx, byc);
                 m.xb = m.xa;
                 m.xb.x = make_map<T>(xb_[l]->p, g, bx, by);
             }
@@ -581,8 +584,8 @@ template <class T, class TC> class VCycle : public VCycleBase {
     void sweep(cudaStream_t s, int l, const T* x_in, T* x_out, const T* e, T* b_coarse, int mode, double* dot_out) {
         const Geom& g = G_[l];
         const bool tma = tma_[l] != 0;
-        const int ty = tma ? tma_ty() : SW_TY;
-        const int gx = (g.nx + SW_TX - 1) / SW_TX, gy = (g.ny + ty - 1) / ty;
+        const int tx = tma ? TmaSweepCfg<T, TC, 0>::TX : SW_TX, ty = tma ? tma_ty() : SW_TY;
+        const int gx = (g.nx + tx - 1) / tx, gy = (g.ny + ty - 1) / ty;
         const T* b = l == 0 ? b0_ : (const T*)bl_[l]->p;
         if (tma) {
             // (tile, z chunk) CTAs, all resident at once: the most chunks per tile that fit
@@ -643,6 +646,9 @@ template <class T, class TC> class VCycle : public VCycleBase {
         using C = TmaSweepCfg<T, TC, MODE>;
         MF3D_CK(cudaFuncSetAttribute(sweep_tma_kernel<T, TC, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)C::SMEM));
+        // all of the unified L1 as shared memory, so that MINB CTAs are co-resident
+        MF3D_CK(cudaFuncSetAttribute(sweep_tma_kernel<T, TC, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared));
         int n = 0;
         MF3D_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_tma_kernel<T, TC, MODE>, C::NT, C::SMEM));
         if (n < 1) throw Error(MF3D_E_CUDA, "staged sweep does not fit on an SM");
