@@ -180,6 +180,46 @@ int mf3d_velocity_mass_balance_noalloc(const mf3d_grid* grid, const mf3d_bc* bc,
                                        const double* K_dev, double* U_dev, double* V_dev,
                                        double* W_dev, double* out_host, void* stream);
 
+/* ---- batched ensemble solves -------------------------------------------------------------
+ * The realisation loop of run_ensemble (src/runtime/ensemble/EnsembleRunner.cu:259-317) calls
+ * solve_head once per realisation.  A batch holds `count` independent head solvers, one grid
+ * each (sizes may differ), with one bc and cfg, and solves them together: batched launches over
+ * every realisation, the whole PCG loop of all realisations in one CUDA graph, and a
+ * per-realisation stopping test (a realisation that has converged does no more work while the
+ * others iterate).  Supported: solver = PCG_MG, mg_pre_smooth >= 1, mg_post_smooth >= 1, and a
+ * hierarchy with at least one level above the coarse tail (grids of 32 cells per axis or more
+ * in practice). */
+typedef struct mf3d_batch mf3d_batch;
+/* Tuning record of one sweep position of the batched V-cycle (mf3d_batch_autotune). */
+typedef struct mf3d_batch_tuning {
+    int phase;        /* 0 pre-smoothing (down), 1 post-smoothing (up) */
+    int level;        /* level depth */
+    int sweep;        /* sweep index, 1-based */
+    int mode;         /* fused stages of the sweep (first-sweep zero guess 1, prolongation 2, residual+restriction 4, <r,z> 8) */
+    int path;         /* 0 staged (TMA) sweep where the level is 16-byte aligned, 1 L1 sweep for all */
+    int chunks;       /* z chunks per tile: the z depth of a work item is nz / chunks */
+    double ms_default;/* device time of the default choice */
+    double ms_best;   /* device time of the choice kept */
+} mf3d_batch_tuning;
+/* EnsembleRunner's per-realisation solver set-up (workspaces.cuh:111-167), for all realisations. */
+int mf3d_batch_create(int count, const mf3d_grid* grids, const mf3d_bc* bc, const mf3d_solver_config* cfg,
+                      void* stream, mf3d_batch** out);
+int mf3d_batch_destroy(mf3d_batch* b);
+int mf3d_batch_count(const mf3d_batch* b);
+long long mf3d_batch_device_bytes(const mf3d_batch* b);
+/* mf3d_head_solver_set_K for every realisation: K_dev[r] is realisation r's K (device). */
+int mf3d_batch_set_K(mf3d_batch* b, const double* const* K_dev);
+/* solve_head for every realisation (EnsembleRunner.cu:286-289): h_dev[r] receives realisation
+ * r's head; x0_dev may be NULL (the reference's guess for all) or hold NULL entries.
+ * results[r] as mf3d_head_solve's; device_ms and kernel_launches are the whole batch's. */
+int mf3d_batch_solve(mf3d_batch* b, double* const* h_dev, const double* const* x0_dev,
+                     mf3d_solve_result* results);
+/* Autotuner (no counterpart in the reference): for every sweep position of the batched
+ * V-cycle, times the candidate work-item shapes (z chunks per tile 1, 2, 4, 8; staged or L1
+ * sweep) on this batch, `reps` launches each, and keeps the fastest.  Fills up to `cap`
+ * records and sets *count.  The solver state is scratch afterwards (the next solve rebuilds it). */
+int mf3d_batch_autotune(mf3d_batch* b, int reps, mf3d_batch_tuning* out, int cap, int* count);
+
 /* ---- operator pieces (device pointers, FP64; in-place where the reference is) ------------- */
 /* VarCoeffLaplacian::apply, src/numerics/operators/varcoeff_laplacian.cu:241-277 */
 int mf3d_apply_A(const mf3d_grid* g, const mf3d_bc* bc, int pin, const double* K, const double* x,

@@ -10,7 +10,7 @@ from __future__ import annotations
 
 import ctypes as C
 from dataclasses import dataclass
-from typing import Optional, Tuple
+from typing import List, Optional, Sequence, Tuple
 
 from . import _lib
 from ._lib import Mf3dError, check, lib
@@ -187,6 +187,72 @@ class HeadSolver:
         """MultigridPreconditioner::apply (src/numerics/solvers/mg_preconditioner.cu:16-44)."""
         n = self.grid.num_cells()
         check(lib().mf3d_head_solver_vcycle(self._h, _f64(r, n, "r"), _f64(z, n, "z")))
+
+
+class BatchSolver:
+    """Independent head solves of several realisations, each on its own grid, solved together
+    (the realisation loop of run_ensemble, src/runtime/ensemble/EnsembleRunner.cu:259-317,
+    without the loop): batched launches, one CUDA graph for the whole PCG loop of all
+    realisations, and a per-realisation stopping test."""
+
+    def __init__(self, grids: Sequence[Grid3D], bc: BCSpec, cfg: Optional[HeadSolveConfig] = None,
+                 stream=None):
+        self.grids = list(grids)
+        self.bc = bc
+        self.cfg = cfg or HeadSolveConfig()
+        arr = (_lib.Grid * len(self.grids))(*[g.c() for g in self.grids])
+        h = C.c_void_p()
+        s = C.c_void_p(stream) if isinstance(stream, int) else (stream or C.c_void_p())
+        check(lib().mf3d_batch_create(len(self.grids), arr, C.byref(_bc(bc)), C.byref(self.cfg.c()), s,
+                                      C.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().mf3d_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self) -> int:
+        return len(self.grids)
+
+    @property
+    def device_bytes(self) -> int:
+        return lib().mf3d_batch_device_bytes(self._h)
+
+    def _ptrs(self, arrays, what, allow_none=False):
+        if len(arrays) != len(self.grids):
+            raise ValueError(f"{what}: expected {len(self.grids)} arrays, got {len(arrays)}")
+        out = (C.c_void_p * len(arrays))()
+        for i, (a, g) in enumerate(zip(arrays, self.grids)):
+            out[i] = None if (a is None and allow_none) else _f64(a, g.num_cells(), f"{what}[{i}]")
+        return out
+
+    def set_K(self, Ks) -> None:
+        check(lib().mf3d_batch_set_K(self._h, self._ptrs(Ks, "K")))
+
+    def solve(self, hs, x0s=None) -> List[HeadSolveResult]:
+        res = (_lib.SolveResult * len(self.grids))()
+        x0p = None if x0s is None else self._ptrs(x0s, "x0", allow_none=True)
+        check(lib().mf3d_batch_solve(self._h, self._ptrs(hs, "h"), x0p, res))
+        return [HeadSolveResult(r.num_iterations, r.initial_residual, r.final_residual, bool(r.converged),
+                                r.status, r.num_levels, r.true_rel_residual, r.b_norm, r.device_ms,
+                                r.kernel_launches) for r in res]
+
+    def autotune(self, reps: int = 3):
+        """Times the candidate work-item shapes of every sweep position of the batched V-cycle
+        and keeps the fastest; returns one dict per sweep position."""
+        cap = 256
+        arr = (_lib.BatchTuning * cap)()
+        cnt = C.c_int(0)
+        check(lib().mf3d_batch_autotune(self._h, int(reps), arr, cap, C.byref(cnt)))
+        return [dict(phase=t.phase, level=t.level, sweep=t.sweep, mode=t.mode, path=t.path, chunks=t.chunks,
+                     ms_default=t.ms_default, ms_best=t.ms_best) for t in arr[:cnt.value]]
 
 
 def solve_head(h, K, grid: Grid3D, bc: BCSpec, cfg: HeadSolveConfig,

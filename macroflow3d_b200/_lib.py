@@ -43,6 +43,12 @@ class KernelTiming(C.Structure):
                 ("launches_per_iter", C.c_int)]
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("phase", C.c_int), ("level", C.c_int), ("sweep", C.c_int), ("mode", C.c_int),
+                ("path", C.c_int), ("chunks", C.c_int), ("ms_default", C.c_double),
+                ("ms_best", C.c_double)]
+
+
 # every symbol include/mf3d.h declares, with its ctypes signature
 _P = C.c_void_p
 _G = C.POINTER(Grid)
@@ -61,6 +67,13 @@ SIGNATURES = {
     "mf3d_head_solver_profile": ([_P, C.c_int, C.POINTER(KernelTiming), C.c_int, C.POINTER(C.c_int)],
                                  C.c_int),
     "mf3d_head_solver_setup_launches": ([_P], C.c_int),
+    "mf3d_batch_create": ([C.c_int, _G, _B, C.POINTER(SolverConfig), _P, C.POINTER(_P)], C.c_int),
+    "mf3d_batch_destroy": ([_P], C.c_int),
+    "mf3d_batch_count": ([_P], C.c_int),
+    "mf3d_batch_device_bytes": ([_P], C.c_longlong),
+    "mf3d_batch_set_K": ([_P, C.POINTER(_P)], C.c_int),
+    "mf3d_batch_solve": ([_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(SolveResult)], C.c_int),
+    "mf3d_batch_autotune": ([_P, C.c_int, C.POINTER(BatchTuning), C.c_int, C.POINTER(C.c_int)], C.c_int),
     "mf3d_velocity_from_head": ([_G, _B, _P, _P, C.c_int, _P, _P, _P, _P], C.c_int),
     "mf3d_velocity_mass_balance": ([_G, _B, _P, _P, _P, _P, _P, C.POINTER(C.c_double), _P], C.c_int),
     "mf3d_velocity_mass_balance_noalloc": ([_G, _B, _P, _P, _P, _P, _P, C.POINTER(C.c_double), _P], C.c_int),

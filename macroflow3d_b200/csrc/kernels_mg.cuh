@@ -37,6 +37,7 @@ template <class T, class TC, class TB> struct SweepArgs {
     unsigned* dot_ticket;
     double* dot_out;
     const double* r64;    // FP64 residual for M_DOT
+    const int* stop;      // batched launches: the realisation's stop flag (skip when set)
 };
 
 __device__ __forceinline__ int pmod(int a, int m) {
@@ -45,7 +46,7 @@ __device__ __forceinline__ int pmod(int a, int m) {
 }
 
 template <class T, class TC, class TB, int MODE>
-__global__ void __launch_bounds__(SW_NT) sweep_kernel(const SweepArgs<T, TC, TB> a) {
+__device__ __forceinline__ void sweep_body(const SweepArgs<T, TC, TB>& a, const VBlk& vb) {
     constexpr bool ZERO = (MODE & M_ZERO) != 0;
     constexpr bool PROL = (MODE & M_PROLONG) != 0;
     constexpr bool RESID = (MODE & M_RESID) != 0;
@@ -60,8 +61,8 @@ __global__ void __launch_bounds__(SW_NT) sweep_kernel(const SweepArgs<T, TC, TB>
     const LevelOp<TC>& L = a.L;
     const int nx = L.nx, ny = L.ny, nz = L.nz;
     const size_t nxy = (size_t)nx * ny;
-    const int i0 = blockIdx.x * SW_TX, j0 = blockIdx.y * SW_TY;
-    const int z0 = blockIdx.z * a.zchunk;
+    const int i0 = vb.x * SW_TX, j0 = vb.y * SW_TY;
+    const int z0 = vb.z * a.zchunk;
     const int z1 = min(z0 + a.zchunk, nz);
     const int tid = threadIdx.x;
     const T dx2 = (T)L.dx2;
@@ -209,9 +210,26 @@ __global__ void __launch_bounds__(SW_NT) sweep_kernel(const SweepArgs<T, TC, TB>
 
     if (DOT) {
         double v[1] = {dot_acc}, out[1];
-        const int nblocks = gridDim.x * gridDim.y * gridDim.z;
-        if (grid_sums<SW_NT, 1>(v, a.dot_partials, a.dot_ticket, nblocks, out)) *a.dot_out = out[0];
+        if (grid_sums<SW_NT, 1>(v, a.dot_partials, a.dot_ticket, vb.count, out, vb.id)) *a.dot_out = out[0];
     }
+}
+
+template <class T, class TC, class TB, int MODE>
+__global__ void __launch_bounds__(SW_NT) sweep_kernel(const SweepArgs<T, TC, TB> a) {
+    sweep_body<T, TC, TB, MODE>(a, hw_vblk());
+}
+
+// The same sweep for several realisations in one launch: segment s (args[s], its block grid
+// dims[s]) owns the CTAs [off[s], off[s+1]); realisations whose solve has stopped are skipped.
+template <class T, class TC, class TB, int MODE>
+__global__ void __launch_bounds__(SW_NT) sweep_batch_kernel(const SweepArgs<T, TC, TB>* __restrict__ args,
+                                                            const int4* __restrict__ dims, const int* __restrict__ off,
+                                                            int nseg) {
+    const int s = find_seg(off, nseg, blockIdx.x);
+    const SweepArgs<T, TC, TB>& a = args[s];
+    if (a.stop && *a.stop) return;
+    const int4 d = dims[s];
+    sweep_body<T, TC, TB, MODE>(a, make_vblk(blockIdx.x - off[s], d.x, d.y, d.z));
 }
 
 // x_out = x_in + P e_c  (or P e_c when x_in is null): the prolongation alone, for levels

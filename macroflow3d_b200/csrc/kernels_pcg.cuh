@@ -41,10 +41,6 @@ __device__ __forceinline__ unsigned long long global_ns() {
 
 constexpr int PK_NT = 256;
 
-__device__ __forceinline__ bool first_thread() {
-    return (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y | threadIdx.z) == 0;
-}
-
 // y = A x with the reference operator (src/numerics/operators/varcoeff_laplacian.cu:38-239):
 // y_c = (sum_f C_f x_f - D_c x_c) / dx^2, and with the pin the diagonal at cell 0 grows by
 // the coefficients of its in-domain faces only (varcoeff_laplacian.cu:225-229).
@@ -75,13 +71,13 @@ __device__ __forceinline__ double apply_A_cell(const LevelOp<TC>& L, const doubl
 // r = b - A x, with ||r||^2 and ||b||^2.  mode 0 (start of solve): fills r0sq, rr, bb,
 // ref_norm and resets the counters; mode 1 (end of solve): fills rr_true, r is scratch.
 template <class TC>
-__global__ void __launch_bounds__(PK_NT) residual_kernel(const LevelOp<TC> L, const double* __restrict__ x,
-                                                         const double* __restrict__ b, double* __restrict__ r,
-                                                         PcgState* st, double* partials, unsigned* ticket,
-                                                         int mode, int ref_is_b, float* __restrict__ r32,
-                                                         cudaGraphConditionalHandle cond, int use_cond, int zchunk) {
+__device__ __forceinline__ void residual_body(const LevelOp<TC>& L, const double* __restrict__ x,
+                                              const double* __restrict__ b, double* __restrict__ r, PcgState* st,
+                                              double* partials, unsigned* ticket, int mode, int ref_is_b,
+                                              float* __restrict__ r32, cudaGraphConditionalHandle cond,
+                                              int use_cond, int zchunk, const VBlk& vb) {
     const bool mg = st->solver == SOLVE_MG;
-    const bool first = first_thread();
+    const bool first = vb.id == 0 && threadIdx.x == 0 && threadIdx.y == 0;
     if (mode == 2 && st->stop) { // standalone MG: finished before this cycle
         if (use_cond && first) cudaGraphSetConditional(cond, 0u);
         return;
@@ -97,7 +93,7 @@ __global__ void __launch_bounds__(PK_NT) residual_kernel(const LevelOp<TC> L, co
         }
     }
     double srr = 0.0, sbb = 0.0;
-    const Col3 q = col3(L.nx, L.ny, L.nz, zchunk);
+    const Col3 q = col3(L.nx, L.ny, L.nz, zchunk, vb.x, vb.y, vb.z);
     if (q.ok) {
         const size_t nxy = (size_t)L.nx * L.ny;
         for (int k = q.k0; k < q.k1; ++k) {
@@ -111,7 +107,7 @@ __global__ void __launch_bounds__(PK_NT) residual_kernel(const LevelOp<TC> L, co
         }
     }
     double v[2] = {srr, sbb}, out[2];
-    if (grid_sums<PK_NT, 2>(v, partials, ticket, gridDim.x * gridDim.y * gridDim.z, out)) {
+    if (grid_sums<PK_NT, 2>(v, partials, ticket, vb.count, out, vb.id)) {
         if (mode == 0) {
             st->r0sq = out[0];
             st->rr = out[0];
@@ -161,32 +157,46 @@ __global__ void __launch_bounds__(PK_NT) residual_kernel(const LevelOp<TC> L, co
     }
 }
 
+template <class TC>
+__global__ void __launch_bounds__(PK_NT) residual_kernel(const LevelOp<TC> L, const double* __restrict__ x,
+                                                         const double* __restrict__ b, double* __restrict__ r,
+                                                         PcgState* st, double* partials, unsigned* ticket,
+                                                         int mode, int ref_is_b, float* __restrict__ r32,
+                                                         cudaGraphConditionalHandle cond, int use_cond, int zchunk) {
+    residual_body<TC>(L, x, b, r, st, partials, ticket, mode, ref_is_b, r32, cond, use_cond, zchunk, hw_vblk());
+}
+
 // p = z + beta p; beta = 0 on the first iteration, Fletcher-Reeves rho_new/rho_old, or the
 // flexible Polak-Ribiere form (rho_new - gamma)/rho_old.
 template <class TZ>
-__global__ void __launch_bounds__(PK_NT) pupdate_kernel(size_t n, const TZ* __restrict__ z, double* __restrict__ p,
-                                                        PcgState* st) {
+__device__ __forceinline__ void pupdate_body(size_t n, const TZ* __restrict__ z, double* __restrict__ p, PcgState* st,
+                                             int blk, int nblk) {
     const PcgState s = *st;
     if (s.stop) return;
     const double beta = s.iter == 0 ? 0.0 : (s.rho_new - (s.flexible ? s.gamma : 0.0)) / s.rho_old;
-    if (blockIdx.x == 0 && threadIdx.x == 0) st->beta = beta;
+    if (blk == 0 && threadIdx.x == 0) st->beta = beta;
     if (s.iter == 0) { // p = z exactly: whatever p held before must not leak in through 0 * p
-        for (size_t c = blockIdx.x * (size_t)PK_NT + threadIdx.x; c < n; c += (size_t)gridDim.x * PK_NT)
-            p[c] = (double)z[c];
+        for (size_t c = blk * (size_t)PK_NT + threadIdx.x; c < n; c += (size_t)nblk * PK_NT) p[c] = (double)z[c];
         return;
     }
-    for (size_t c = blockIdx.x * (size_t)PK_NT + threadIdx.x; c < n; c += (size_t)gridDim.x * PK_NT)
+    for (size_t c = blk * (size_t)PK_NT + threadIdx.x; c < n; c += (size_t)nblk * PK_NT)
         p[c] = 1.0 * (double)z[c] + beta * p[c];
+}
+
+template <class TZ>
+__global__ void __launch_bounds__(PK_NT) pupdate_kernel(size_t n, const TZ* __restrict__ z, double* __restrict__ p,
+                                                        PcgState* st) {
+    pupdate_body<TZ>(n, z, p, st, blockIdx.x, gridDim.x);
 }
 
 // Ap = A p and <p, Ap>.
 template <class TC>
-__global__ void __launch_bounds__(PK_NT) matvec_dot_kernel(const LevelOp<TC> L, const double* __restrict__ p,
-                                                           double* __restrict__ Ap, PcgState* st,
-                                                           double* partials, unsigned* ticket, int zchunk) {
+__device__ __forceinline__ void matvec_dot_body(const LevelOp<TC>& L, const double* __restrict__ p,
+                                                double* __restrict__ Ap, PcgState* st, double* partials,
+                                                unsigned* ticket, int zchunk, const VBlk& vb) {
     if (st->stop) return;
     double acc = 0.0;
-    const Col3 q = col3(L.nx, L.ny, L.nz, zchunk);
+    const Col3 q = col3(L.nx, L.ny, L.nz, zchunk, vb.x, vb.y, vb.z);
     if (q.ok) {
         const size_t nxy = (size_t)L.nx * L.ny;
         for (int k = q.k0; k < q.k1; ++k) {
@@ -197,21 +207,27 @@ __global__ void __launch_bounds__(PK_NT) matvec_dot_kernel(const LevelOp<TC> L, 
         }
     }
     double v[1] = {acc}, out[1];
-    if (grid_sums<PK_NT, 1>(v, partials, ticket, gridDim.x * gridDim.y * gridDim.z, out)) st->pAp = out[0];
+    if (grid_sums<PK_NT, 1>(v, partials, ticket, vb.count, out, vb.id)) st->pAp = out[0];
+}
+
+template <class TC>
+__global__ void __launch_bounds__(PK_NT) matvec_dot_kernel(const LevelOp<TC> L, const double* __restrict__ p,
+                                                           double* __restrict__ Ap, PcgState* st,
+                                                           double* partials, unsigned* ticket, int zchunk) {
+    matvec_dot_body<TC>(L, p, Ap, st, partials, ticket, zchunk, hw_vblk());
 }
 
 // x += alpha p; r -= alpha Ap (alpha = rho_new / pAp); ||r||^2 and, for the flexible form,
 // gamma = <r_{k+1}, z_k>.  The last CTA runs the stopping test of pcg.cuh:156-164 and sets
 // the graph's while condition.
 template <class TZ>
-__global__ void __launch_bounds__(PK_NT) xr_update_kernel(size_t n, double* __restrict__ x, const double* __restrict__ p,
-                                                          double* __restrict__ r, const double* __restrict__ Ap,
-                                                          const TZ* __restrict__ z, PcgState* st,
-                                                          double* partials, unsigned* ticket,
-                                                          cudaGraphConditionalHandle cond, int use_cond,
-                                                          float* __restrict__ r32) {
+__device__ __forceinline__ void xr_update_body(size_t n, double* __restrict__ x, const double* __restrict__ p,
+                                               double* __restrict__ r, const double* __restrict__ Ap,
+                                               const TZ* __restrict__ z, PcgState* st, double* partials,
+                                               unsigned* ticket, cudaGraphConditionalHandle cond, int use_cond,
+                                               float* __restrict__ r32, int blk, int nblk) {
     const PcgState s = *st;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (blk == 0 && threadIdx.x == 0) {
         // Loop bound that does not depend on the reductions: a body count and a device-time
         // budget, both checked by one thread, so no failure elsewhere can keep the loop alive.
         const int bc = atomicAdd(&st->body_count, 1) + 1;
@@ -223,12 +239,12 @@ __global__ void __launch_bounds__(PK_NT) xr_update_kernel(size_t n, double* __re
         }
     }
     if (s.stop) { // converged or failed before this iteration: leave x, r alone and end the loop
-        if (use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0u);
+        if (use_cond && blk == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0u);
         return;
     }
     const double alpha = s.rho_new / s.pAp;
     double srr = 0.0, sg = 0.0;
-    for (size_t c = blockIdx.x * (size_t)PK_NT + threadIdx.x; c < n; c += (size_t)gridDim.x * PK_NT) {
+    for (size_t c = blk * (size_t)PK_NT + threadIdx.x; c < n; c += (size_t)nblk * PK_NT) {
         x[c] = x[c] + alpha * p[c];
         const double rv = r[c] + (-alpha) * Ap[c];
         r[c] = rv;
@@ -237,7 +253,7 @@ __global__ void __launch_bounds__(PK_NT) xr_update_kernel(size_t n, double* __re
         if (s.flexible) sg += rv * (double)z[c];
     }
     double v[2] = {srr, sg}, out[2];
-    if (grid_sums<PK_NT, 2>(v, partials, ticket, gridDim.x, out)) {
+    if (grid_sums<PK_NT, 2>(v, partials, ticket, nblk, out, blk)) {
         const int it = s.iter + 1;
         st->iter = it;
         st->alpha = alpha;
@@ -266,6 +282,16 @@ __global__ void __launch_bounds__(PK_NT) xr_update_kernel(size_t n, double* __re
         st->stop = stop;
         if (use_cond) cudaGraphSetConditional(cond, stop ? 0u : 1u);
     }
+}
+
+template <class TZ>
+__global__ void __launch_bounds__(PK_NT) xr_update_kernel(size_t n, double* __restrict__ x, const double* __restrict__ p,
+                                                          double* __restrict__ r, const double* __restrict__ Ap,
+                                                          const TZ* __restrict__ z, PcgState* st,
+                                                          double* partials, unsigned* ticket,
+                                                          cudaGraphConditionalHandle cond, int use_cond,
+                                                          float* __restrict__ r32) {
+    xr_update_body<TZ>(n, x, p, r, Ap, z, st, partials, ticket, cond, use_cond, r32, blockIdx.x, gridDim.x);
 }
 
 // Sets the while condition before the loop from the state left by residual_kernel(mode 0).

@@ -73,6 +73,14 @@ template <class T, class TC> struct TmaSweepArgs {
     double* dot_out;
     int zchunk; // planes per CTA (even)
     int* err;   // set to 1 when an mbarrier wait gives up
+    const int* stop; // batched launches: the realisation's stop flag (its items are skipped)
+    // batched launches, the launch-wide argument only: work items [seg_off[s], seg_off[s+1])
+    // belong to realisation segment s, whose arguments and tensor maps are seg_args[s] and
+    // seg_maps[s] (device memory, 64-byte aligned)
+    const int* seg_off;
+    const TmaSweepArgs* seg_args;
+    const TmaMaps* seg_maps;
+    int nseg, total;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -262,9 +270,11 @@ template <class T> struct BlackCoef {
     T b[2], cxp[2], cxm[2], cyp[2], cym[2], czp[2];
 };
 
-template <class T, class TC, int MODE>
+// BATCH: one launch sweeps the same level depth of several realisations; the persistent CTAs
+// walk the concatenated (tile, z chunk) items of every realisation whose solve is running.
+template <class T, class TC, int MODE, bool BATCH = false>
 __global__ void __launch_bounds__(TmaSweepCfg<T, TC, MODE>::NT, TmaSweepCfg<T, TC, MODE>::MINB)
-    sweep_tma_kernel(const __grid_constant__ TmaMaps maps, const TmaSweepArgs<T, TC> a) {
+    sweep_tma_kernel(const __grid_constant__ TmaMaps maps0, const TmaSweepArgs<T, TC> a0) {
     using C = TmaSweepCfg<T, TC, MODE>;
     constexpr bool ZERO = C::ZERO, PROL = C::PROL, RESID = C::RESID;
     constexpr bool DOT = (MODE & M_DOT) != 0;
@@ -283,18 +293,12 @@ __global__ void __launch_bounds__(TmaSweepCfg<T, TC, MODE>::NT, TmaSweepCfg<T, T
     auto xsl = [&](int s) { return reinterpret_cast<T*>(sweep_sm + C::OFF_X + C::XS * s); };
     auto cbase = [&](int s) { return sweep_sm + C::OFF_C + C::CS * s; };
 
-    const LevelOp<TC>& L = a.L;
-    const int nx = L.nx, ny = L.ny, nz = L.nz;
-    const size_t nxy = (size_t)nx * ny;
     const int tid = threadIdx.x;
-    const T dx2 = (T)L.dx2, inv_dx2 = (T)L.inv_dx2;
     auto divide = [](T num, T den) -> T {
         if constexpr (sizeof(T) == 4) return __fdividef(num, den); // preconditioner: 2-ulp division
         else return num / den;
     };
     auto tc = [](TC v) -> T { return ld_as_float_or_double<T>(v); };
-
-    const int ntx = (nx + TX - 1) / TX, nty = (ny + TY - 1) / TY, ntiles = ntx * nty;
 
     if (tid == 0) {
         for (int s = 0; s < 2 * (NRX + NRC); ++s) mbar_init(&barx[s], 1);
@@ -366,9 +370,16 @@ __global__ void __launch_bounds__(TmaSweepCfg<T, TC, MODE>::NT, TmaSweepCfg<T, T
     const int e = (ir - C::RI + H) * BX + C::Q0 + 4 * qc_;     // x (and cy) box element of cell 0
     const int eC = e - (H - RR) * BX;                          // b, cx, cz box element of cell 0
 
-    // CTA b: tile b % ntiles, z chunk b / ntiles (tiles fastest, so neighbouring tiles march
-    // the same planes at the same time and share their halo rows in L2)
-    for (int b = blockIdx.x; b < ntiles * ((nz + a.zchunk - 1) / a.zchunk) && !fail; b += gridDim.x) {
+    // Work item b of a level (nitems items): tile b % ntiles, z chunk b / ntiles (tiles
+    // fastest, so neighbouring tiles march the same planes at the same time and share their
+    // halo rows in L2).
+    auto run_item = [&](const TmaSweepArgs<T, TC>& a, const TmaMaps& maps, const int b, const int nitems) {
+        const LevelOp<TC>& L = a.L;
+        const int nx = L.nx, ny = L.ny, nz = L.nz;
+        const size_t nxy = (size_t)nx * ny;
+        const T dx2 = (T)L.dx2, inv_dx2 = (T)L.inv_dx2;
+        const int ntx = (nx + TX - 1) / TX, ntiles = ntx * ((ny + TY - 1) / TY);
+        (void)nitems;
         // ---------------- one z chunk of one tile ----------------
         const int tile = b % ntiles;
         const int z0 = (b / ntiles) * a.zchunk;
@@ -387,6 +398,14 @@ __global__ void __launch_bounds__(TmaSweepCfg<T, TC, MODE>::NT, TmaSweepCfg<T, T
             // ---- producer: both rings in order of need (x plane p is read one step before
             // coefficient plane p), each copy into a slot the consumers have released ----
             if (tid == C::NCONS) {
+                if constexpr (BATCH) {
+                    // tensor maps read from global memory: order them before their use by TMA
+                    const CUtensorMap* mp[8] = {&maps.x, &maps.b, &maps.cx, &maps.cy, &maps.cz,
+                                                &maps.bxm, &maps.bym, &maps.bzm};
+#pragma unroll
+                    for (int k = 0; k < 8; ++k)
+                        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(mp[k]) : "memory");
+                }
                 auto issue_x = [&](int p) {
                     const unsigned n = qx + (unsigned)(p - pl0);
                     const int s = (int)(n % NRX);
@@ -429,7 +448,7 @@ __global__ void __launch_bounds__(TmaSweepCfg<T, TC, MODE>::NT, TmaSweepCfg<T, T
             }
             if (!ZERO) qx += (unsigned)(xl1 - pl0 + 1);
             qc += (unsigned)(cl1 - pl0 + 1);
-            continue;
+            return;
         }
         // ---- consumers ----
         int xw_plane = pl0, cw_plane = pl0; // thread 0: next plane to wait for
@@ -785,7 +804,7 @@ __global__ void __launch_bounds__(TmaSweepCfg<T, TC, MODE>::NT, TmaSweepCfg<T, T
                 for (int k = nx_done; k < issued[0]; ++k) (void)wait_x();
                 for (int k = nc_done; k < issued[1]; ++k) (void)wait_c();
             }
-            break;
+            return;
         }
         // release the planes still held, so that the producer can reuse their slots
         if (tid == 0) {
@@ -795,11 +814,49 @@ __global__ void __launch_bounds__(TmaSweepCfg<T, TC, MODE>::NT, TmaSweepCfg<T, T
         }
         if (!ZERO) qx += (unsigned)(xl1 - pl0 + 1);
         qc += (unsigned)(cl1 - pl0 + 1);
-    }
+        if constexpr (BATCH && DOT) {
+            // this item's share of <r64, x_out>, summed by the consumers alone (the producer
+            // warp is already issuing the next item); the last item of the realisation adds
+            // the items' partials in index order
+            __shared__ double item_red[C::NCONS / 32];
+            double v = dot_acc;
+            dot_acc = 0.0;
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) item_red[warp] = v;
+            asm volatile("bar.sync 2, %0;" ::"r"(C::NCONS) : "memory");
+            if (tid == 0) {
+                double sum = 0.0;
+                for (int w = 0; w < C::NCONS / 32; ++w) sum += item_red[w];
+                a.dot_partials[b] = sum;
+                __threadfence();
+                if (atomicAdd(a.dot_ticket, 1u) == (unsigned)nitems - 1) {
+                    __threadfence();
+                    double acc = 0.0;
+                    for (int i = 0; i < nitems; ++i) acc += __ldcg(a.dot_partials + i);
+                    *a.dot_out = acc;
+                    *a.dot_ticket = 0u;
+                }
+            }
+            asm volatile("bar.sync 2, %0;" ::"r"(C::NCONS) : "memory");
+        }
+    };
 
-    if (DOT) { // every thread, the producer warp included (grid_sums synchronises the CTA)
-        double v[1] = {dot_acc}, out[1];
-        if (grid_sums<C::NT, 1>(v, a.dot_partials, a.dot_ticket, gridDim.x, out)) *a.dot_out = out[0];
+    if constexpr (BATCH) {
+        for (int b = blockIdx.x; b < a0.total && !fail; b += gridDim.x) {
+            const int sg = find_seg(a0.seg_off, a0.nseg, b);
+            const TmaSweepArgs<T, TC>& A = a0.seg_args[sg];
+            if (A.stop && *A.stop) continue; // that realisation's solve has finished
+            const int o = __ldg(a0.seg_off + sg);
+            run_item(A, a0.seg_maps[sg], b - o, __ldg(a0.seg_off + sg + 1) - o);
+        }
+    } else {
+        const int ntiles = ((a0.L.nx + TX - 1) / TX) * ((a0.L.ny + TY - 1) / TY);
+        const int total = ntiles * ((a0.L.nz + a0.zchunk - 1) / a0.zchunk);
+        for (int b = blockIdx.x; b < total && !fail; b += gridDim.x) run_item(a0, maps0, b, total);
+        if (DOT) { // every thread, the producer warp included (grid_sums synchronises the CTA)
+            double v[1] = {dot_acc}, out[1];
+            if (grid_sums<C::NT, 1>(v, a0.dot_partials, a0.dot_ticket, gridDim.x, out)) *a0.dot_out = out[0];
+        }
     }
 }
 

@@ -117,8 +117,7 @@ __device__ __forceinline__ void tl_smooth(const TailLevel& L, double* x, const d
 }
 
 template <class TI, class TO>
-__global__ void __launch_bounds__(TAIL2_NT, 1) tail2_kernel(const Tail2Args a, const TI* __restrict__ b_in,
-                                                            TO* __restrict__ x_out) {
+__device__ __forceinline__ void tail2_body(const Tail2Args& a, const TI* __restrict__ b_in, TO* __restrict__ x_out) {
     extern __shared__ double sm[];
     const int tid = threadIdx.x;
     // zero every padded x (ghosts included), load b of the top level
@@ -188,6 +187,29 @@ __global__ void __launch_bounds__(TAIL2_NT, 1) tail2_kernel(const Tail2Args a, c
             x_out[c] = (TO)sm[L.xoff + tl_pad(L, i, j, k)];
         }
     }
+}
+
+template <class TI, class TO>
+__global__ void __launch_bounds__(TAIL2_NT, 1) tail2_kernel(const Tail2Args a, const TI* __restrict__ b_in,
+                                                            TO* __restrict__ x_out) {
+    tail2_body<TI, TO>(a, b_in, x_out);
+}
+
+// One realisation's coarse tail in a batched launch.
+template <class TI, class TO> struct TailItem {
+    Tail2Args a;
+    const TI* b_in;
+    TO* x_out;
+    const int* stop; // skip when set
+};
+
+// The coarse tails of several realisations, one CTA each (the launch's dynamic shared memory
+// is the largest of theirs).
+template <class TI, class TO>
+__global__ void __launch_bounds__(TAIL2_NT, 1) tail2_batch_kernel(const TailItem<TI, TO>* __restrict__ items) {
+    const TailItem<TI, TO>& it = items[blockIdx.x];
+    if (it.stop && *it.stop) return;
+    tail2_body<TI, TO>(it.a, it.b_in, it.x_out);
 }
 
 } // namespace mf3d

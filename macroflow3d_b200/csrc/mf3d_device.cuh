@@ -117,14 +117,16 @@ __device__ __forceinline__ double block_sum(double v, double* red /* NT/32 doubl
 }
 
 // Returns true on thread 0 of the last block to finish; `out` then holds the grid sums.
-// Blocks may be 1-, 2- or 3-D; NT is the number of threads per block.
+// Blocks may be 1-, 2- or 3-D; NT is the number of threads per block.  `bid` is the block's
+// index among the `nblocks` that share the partials (the hardware block index by default; a
+// virtual block of one realisation in the batched kernels).
 template <int NT, int NV>
 __device__ __forceinline__ bool grid_sums(const double (&v)[NV], double* partials, unsigned* ticket,
-                                          int nblocks, double (&out)[NV]) {
+                                          int nblocks, double (&out)[NV], int bid = -1) {
     __shared__ double red[NT / 32];
     __shared__ bool s_last;
     const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
-    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    if (bid < 0) bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     for (int q = 0; q < NV; ++q) {
         double s = block_sum<NT>(v[q], red);
         if (tid == 0) partials[(size_t)q * nblocks + bid] = s;
@@ -152,14 +154,59 @@ struct Col3 {
     int i, j, k0, k1;
     bool ok;
 };
-__device__ __forceinline__ Col3 col3(int nx, int ny, int nz, int zchunk) {
+__device__ __forceinline__ Col3 col3(int nx, int ny, int nz, int zchunk, int bx, int by, int bz) {
     Col3 c;
-    c.i = blockIdx.x * 32 + threadIdx.x;
-    c.j = blockIdx.y * 8 + threadIdx.y;
-    c.k0 = blockIdx.z * zchunk;
+    c.i = bx * 32 + threadIdx.x;
+    c.j = by * 8 + threadIdx.y;
+    c.k0 = bz * zchunk;
     c.k1 = min(c.k0 + zchunk, nz);
     c.ok = c.i < nx && c.j < ny;
     return c;
+}
+__device__ __forceinline__ Col3 col3(int nx, int ny, int nz, int zchunk) {
+    return col3(nx, ny, nz, zchunk, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// ---------------------------------------------------------------------------------------
+// Batched launches.  One launch serves several independent realisations ("segments"): the
+// virtual blocks of segment s are [off[s], off[s+1]) and a CTA finds its segment by binary
+// search.  A virtual block is a 3-D block index (x fastest) of that segment's own grid.
+// ---------------------------------------------------------------------------------------
+struct VBlk {
+    int x, y, z;    // block index in the segment's grid
+    int gx, gy, gz; // the segment's grid
+    int id, count;  // linear index and number of blocks
+};
+
+__device__ __forceinline__ VBlk hw_vblk() {
+    VBlk v;
+    v.x = blockIdx.x, v.y = blockIdx.y, v.z = blockIdx.z;
+    v.gx = gridDim.x, v.gy = gridDim.y, v.gz = gridDim.z;
+    v.id = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    v.count = gridDim.x * gridDim.y * gridDim.z;
+    return v;
+}
+
+__device__ __forceinline__ VBlk make_vblk(int id, int gx, int gy, int gz) {
+    VBlk v;
+    v.id = id;
+    v.gx = gx, v.gy = gy, v.gz = gz;
+    v.count = gx * gy * gz;
+    v.x = id % gx;
+    v.y = (id / gx) % gy;
+    v.z = id / (gx * gy);
+    return v;
+}
+
+// segment of virtual block b: the last s with off[s] <= b (off[0] = 0, off[nseg] = total)
+__device__ __forceinline__ int find_seg(const int* __restrict__ off, int nseg, int b) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(off + mid) <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
 }
 
 } // namespace mf3d

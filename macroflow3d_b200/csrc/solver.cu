@@ -372,8 +372,10 @@ template <class T, class TC> class VCycle : public VCycleBase {
                               bc.type[4] == MF3D_BC_PERIODIC;
         for (int l = 0; l < Lt && allow_tma && !periodic; ++l) {
             const Geom& g = G[l];
-            if ((g.nx * sizeof(T)) % 16 || (g.nx * sizeof(TC)) % 16 || (g.ny * sizeof(TC)) % 16 || g.nx < 16 ||
-                g.ny < 8)
+            // TMA boxes start on 16-byte boundaries, and the staged sweep's 4-cell quads need
+            // nx to be a multiple of 4 (a quad is all inside the grid or all outside)
+            if ((g.nx * sizeof(T)) % 16 || (g.nx * sizeof(TC)) % 16 || (g.ny * sizeof(TC)) % 16 || g.nx % 4 ||
+                g.nx < 16 || g.ny < 8)
                 continue;
             tma_[l] = 1;
             ++n_tma_;
@@ -439,6 +441,30 @@ template <class T, class TC> class VCycle : public VCycleBase {
         }
     }
 
+    // ---- batched solves: run() with rec_ / rec_tail_ set records its sweeps and its coarse
+    // tail instead of launching them ----
+    struct RecSweep {
+        int phase, level, sw, mode; // phase 0: down (pre-smoothing), 1: up (post-smoothing)
+        bool tma;                   // the staged (TMA) form exists
+        TmaSweepArgs<T, TC> ta;     // staged form, z chunk unset
+        const TmaMaps* maps;
+        SweepArgs<T, TC, T> la; // L1 form, z chunk unset
+        Geom g;
+    };
+    struct RecTail {
+        Tail2Args a;
+        const T* b;
+        T* out;
+        size_t smem;
+    };
+    std::vector<RecSweep>* rec_ = nullptr;
+    RecTail* rec_tail_ = nullptr;
+    int rec_phase_ = 0, rec_sw_ = 0;
+    int levels_above_tail() const { return Lt_; }
+    const Scratch& scratch() const { return scr_; }
+    int pre() const { return pre_; }
+    int post() const { return post_; }
+
     void build_coefs(cudaStream_t s, const std::vector<const double*>& Klev) override {
         if (!std::is_same<TC, double>::value)
             for (int l = 0; l < Lt_; ++l) launch_faces<TC>(s, G_[l], Klev[l], bc_, scale_[l], ops_[l]);
@@ -463,6 +489,8 @@ template <class T, class TC> class VCycle : public VCycleBase {
             for (int sw = 1; sw <= pre_; ++sw) {
                 T* out = other(l, c);
                 int mode = (c ? 0 : M_ZERO) | (sw == pre_ ? M_RESID : 0);
+                rec_phase_ = 0;
+                rec_sw_ = sw;
                 sweep(s, l, c, out, nullptr, bc_next, mode, nullptr);
                 c = out;
             }
@@ -485,6 +513,8 @@ template <class T, class TC> class VCycle : public VCycleBase {
                 const bool last = sw == post_;
                 T* out = (l == 0 && last) ? z : other(l, c);
                 int mode = (c ? 0 : M_ZERO) | (sw == 1 ? M_PROLONG : 0) | ((l == 0 && last && rho_out) ? M_DOT : 0);
+                rec_phase_ = 1;
+                rec_sw_ = sw;
                 sweep(s, l, c, out, e, nullptr, mode, rho_out);
                 c = out;
             }
@@ -566,6 +596,14 @@ template <class T, class TC> class VCycle : public VCycleBase {
     T* other(int l, const T* c) const { return (c == (const T*)xa_[l]->p) ? (T*)xb_[l]->p : (T*)xa_[l]->p; }
 
     void launch_tail(cudaStream_t s, T* out) {
+        if (rec_tail_) { // batched solve: record only (the batch needs a level above the tail)
+            if (Lt_ == 0) throw Error(MF3D_E_INVALID, "batched solve: the whole hierarchy fits the coarse tail");
+            rec_tail_->a = tail_;
+            rec_tail_->b = (const T*)bl_[Lt_]->p;
+            rec_tail_->out = out;
+            rec_tail_->smem = tail_smem_;
+            return;
+        }
         if (Lt_ == 0)
             tail2_kernel<double, T><<<1, TAIL2_NT, tail_smem_, s>>>(tail_, r64_, out);
         else
@@ -581,12 +619,69 @@ template <class T, class TC> class VCycle : public VCycleBase {
         return std::min(zc, ((g.nz + 1) & ~1));
     }
 
+    // arguments of the staged (TMA) sweep of level l, but for its z chunk; *maps the tensor
+    // maps of the input buffer
+    TmaSweepArgs<T, TC> tma_args(int l, const T* x_in, T* x_out, const T* e, T* b_coarse, int mode, double* dot_out,
+                                 const TmaMaps** maps) const {
+        TmaSweepArgs<T, TC> a{};
+        a.L = ops_[l];
+        a.x_out = x_out;
+        a.e_c = e;
+        if (l + 1 < (int)G_.size()) {
+            a.ncx = G_[l + 1].nx;
+            a.ncy = G_[l + 1].ny;
+        }
+        a.b_coarse = b_coarse;
+        a.r64 = r64_;
+        a.dot_partials = scr_.partials;
+        a.dot_ticket = scr_.tickets + 0;
+        a.dot_out = dot_out;
+        a.err = scr_.err;
+        const Maps4& m4 = maps_[l][(mode & M_RESID) ? 1 : 0];
+        *maps = (x_in == (const T*)xb_[l]->p) ? &m4.xb : &m4.xa;
+        if (x_in && x_in != (const T*)xa_[l]->p && x_in != (const T*)xb_[l]->p)
+            throw Error(MF3D_E_INVALID, "sweep input is not a level buffer");
+        return a;
+    }
+
+    // arguments of the L1-path sweep of level l, but for its z chunk
+    SweepArgs<T, TC, T> ldg_args(int l, const T* x_in, T* x_out, const T* e, T* b_coarse, double* dot_out) const {
+        SweepArgs<T, TC, T> a{};
+        a.L = ops_[l];
+        a.b = l == 0 ? b0_ : (const T*)bl_[l]->p;
+        a.x_in = x_in;
+        a.x_out = x_out;
+        a.e_c = e;
+        if (l + 1 < (int)G_.size()) {
+            a.ncx = G_[l + 1].nx;
+            a.ncy = G_[l + 1].ny;
+        }
+        a.b_coarse = b_coarse;
+        a.dot_partials = scr_.partials;
+        a.dot_ticket = scr_.tickets + 0;
+        a.dot_out = dot_out;
+        a.r64 = r64_;
+        return a;
+    }
+
     void sweep(cudaStream_t s, int l, const T* x_in, T* x_out, const T* e, T* b_coarse, int mode, double* dot_out) {
         const Geom& g = G_[l];
         const bool tma = tma_[l] != 0;
+        if (rec_) { // batched solve: record both forms, launch nothing
+            RecSweep r{};
+            r.phase = rec_phase_;
+            r.level = l;
+            r.sw = rec_sw_;
+            r.mode = mode;
+            r.g = g;
+            r.tma = tma;
+            if (tma) r.ta = tma_args(l, x_in, x_out, e, b_coarse, mode, dot_out, &r.maps);
+            r.la = ldg_args(l, x_in, x_out, e, b_coarse, dot_out);
+            rec_->push_back(r);
+            return;
+        }
         const int tx = tma ? TmaSweepCfg<T, TC, 0>::TX : SW_TX, ty = tma ? tma_ty() : SW_TY;
         const int gx = (g.nx + tx - 1) / tx, gy = (g.ny + ty - 1) / ty;
-        const T* b = l == 0 ? b0_ : (const T*)bl_[l]->p;
         if (tma) {
             // (tile, z chunk) CTAs, all resident at once: the most chunks per tile that fit
             const long long ntiles = (long long)gx * gy;
@@ -596,26 +691,10 @@ template <class T, class TC> class VCycle : public VCycleBase {
             const long long nblk = ntiles * ((g.nz + zc - 1) / zc);
             const dim3 grid((unsigned)std::min(nblk, std::max(resident, ntiles)));
             if ((mode & M_DOT) && grid.x > scr_.partial_cap) throw Error(MF3D_E_INVALID, "reduction scratch too small");
-            TmaSweepArgs<T, TC> a{};
-            a.L = ops_[l];
-            a.x_out = x_out;
-            a.e_c = e;
-            if (l + 1 < (int)G_.size()) {
-                a.ncx = G_[l + 1].nx;
-                a.ncy = G_[l + 1].ny;
-            }
-            a.b_coarse = b_coarse;
+            const TmaMaps* maps = nullptr;
+            TmaSweepArgs<T, TC> a = tma_args(l, x_in, x_out, e, b_coarse, mode, dot_out, &maps);
             a.zchunk = zc;
-            a.r64 = r64_;
-            a.dot_partials = scr_.partials;
-            a.dot_ticket = scr_.tickets + 0;
-            a.dot_out = dot_out;
-            a.err = scr_.err;
-            const Maps4& m4 = maps_[l][(mode & M_RESID) ? 1 : 0];
-            const TmaMaps& maps = (x_in == (const T*)xb_[l]->p) ? m4.xb : m4.xa;
-            if (x_in && x_in != (const T*)xa_[l]->p && x_in != (const T*)xb_[l]->p)
-                throw Error(MF3D_E_INVALID, "sweep input is not a level buffer");
-            dispatch_tma(s, grid, mode, maps, a);
+            dispatch_tma(s, grid, mode, *maps, a);
             return;
         }
         const int zc = zchunk_for(g, gx * gy, num_sms() * 6);
@@ -623,22 +702,8 @@ template <class T, class TC> class VCycle : public VCycleBase {
         dim3 grid(gx, gy, gz);
         const unsigned nblk = (unsigned)gx * gy * gz;
         if ((mode & M_DOT) && nblk > scr_.partial_cap) throw Error(MF3D_E_INVALID, "reduction scratch too small");
-        SweepArgs<T, TC, T> a{};
-        a.L = ops_[l];
-        a.b = b;
-        a.x_in = x_in;
-        a.x_out = x_out;
-        a.e_c = e;
-        if (l + 1 < (int)G_.size()) {
-            a.ncx = G_[l + 1].nx;
-            a.ncy = G_[l + 1].ny;
-        }
-        a.b_coarse = b_coarse;
+        SweepArgs<T, TC, T> a = ldg_args(l, x_in, x_out, e, b_coarse, dot_out);
         a.zchunk = zc;
-        a.dot_partials = scr_.partials;
-        a.dot_ticket = scr_.tickets + 0;
-        a.dot_out = dot_out;
-        a.r64 = r64_;
         dispatch(s, grid, mode, a);
     }
 
@@ -760,10 +825,14 @@ void VCycle<T, TC>::dot_rz(cudaStream_t s, const T* z, size_t n, double* out) {
     MF3D_LAUNCH_CK();
 }
 
+template <class T, class TC> class BatchSolverT;
+
 // ---------------------------------------------------------------------------------------
 // HeadSolver
 // ---------------------------------------------------------------------------------------
 class HeadSolver {
+    template <class T, class TC> friend class BatchSolverT;
+
   public:
     HeadSolver(const mf3d_grid& g, const mf3d_bc& bc, const mf3d_solver_config& cfg, cudaStream_t user_stream)
         : grid_(g), bc_(bc), cfg_(cfg) {
@@ -1724,3 +1793,5 @@ int mf3d_kfield_eval(const mf3d_grid* g, int n_modes, const double* modes, doubl
 }
 
 } // extern "C"
+
+#include "batch.cuh"

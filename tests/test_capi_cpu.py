@@ -56,6 +56,29 @@ def test_invalid_arguments_return_status(mf3d):
         == _lib.MF3D_E_INVALID
 
 
+def test_batch_refuses_bad_arguments_before_any_device_call(mf3d):
+    from macroflow3d_b200 import _lib
+    L = _lib.lib()
+    h = C.c_void_p()
+    grids = (_lib.Grid * 2)(_lib.Grid(32, 32, 32, 1.0), _lib.Grid(0, 32, 32, 1.0))
+    bc = _lib.BC()
+    cfg = _lib.SolverConfig()
+    L.mf3d_default_config(C.byref(cfg))
+    assert L.mf3d_batch_create(0, grids, C.byref(bc), C.byref(cfg), None, C.byref(h)) == _lib.MF3D_E_INVALID
+    assert b"count" in L.mf3d_last_error()
+    assert L.mf3d_batch_create(2, grids, C.byref(bc), C.byref(cfg), None, C.byref(h)) == _lib.MF3D_E_INVALID
+    grids[1] = _lib.Grid(48, 32, 32, 1.0)
+    cfg.solver = 2  # plain CG: not batched
+    assert L.mf3d_batch_create(2, grids, C.byref(bc), C.byref(cfg), None, C.byref(h)) == _lib.MF3D_E_INVALID
+    assert b"PCG_MG" in L.mf3d_last_error()
+    cfg.solver = 0
+    cfg.mg_post_smooth = 0
+    assert L.mf3d_batch_create(2, grids, C.byref(bc), C.byref(cfg), None, C.byref(h)) == _lib.MF3D_E_INVALID
+    assert not h.value
+    assert L.mf3d_batch_solve(None, None, None, None) == _lib.MF3D_E_INVALID
+    assert L.mf3d_batch_device_bytes(None) == -1
+
+
 def test_kfield_modes_deterministic_and_distributed(mf3d):
     m1 = mf3d.kfield_modes(1234, 4000, mf3d.COV_EXPONENTIAL, (4.0, 4.0, 4.0))
     m2 = mf3d.kfield_modes(1234, 4000, mf3d.COV_EXPONENTIAL, (4.0, 4.0, 4.0))

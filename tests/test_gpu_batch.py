@@ -1,0 +1,205 @@
+"""Batched ensemble solves (mf3d_batch_*) against one HeadSolver per realisation.
+
+The batch replaces the realisation loop of run_ensemble (src/runtime/ensemble/
+EnsembleRunner.cu:259-317), so every realisation must come out as its own single solve would:
+same iteration count (the batch changes only the summation order of the in-sweep <r, z>), the
+same head to well below the solve tolerance, and the per-realisation stopping test must freeze
+a realisation once it has converged while the others iterate.  Grids are uneven on purpose:
+different level counts, levels with and without a staged (TMA) form, non-cubic coarse grids.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+# both arms stop at ||r||/||b|| <= 1e-10; their iterates differ by rounding only
+HEAD_TOL = 1e-8
+# after a fixed number of iterations the iterates agree to rounding (the batch sums the
+# in-sweep <r, z> per work item, the single solve per CTA)
+ITERATE_TOL = 1e-10
+# near the stopping threshold the plain FP64 method (Fletcher-Reeves beta with the reference's
+# non-symmetric V-cycle) converges unevenly, so a rounding difference can move the stop by an
+# iteration or two; the flexible mixed-precision method does not
+ITER_SLACK = {"fp32": 1, "bf16": 1, "fp64": 2}
+
+
+def _grids(M):
+    # 36: level 1 is 18 wide (not 16-byte aligned: L1 sweep); 48x40x24: three sweep levels
+    shapes = [(32, 32, 32), (48, 40, 24), (36, 32, 32), (64, 32, 48), (32, 64, 40)]
+    return [M.Grid3D(nx, ny, nz, 1.0) for nx, ny, nz in shapes]
+
+
+def _cfg(M, prec, **kw):
+    c = dict(mg_levels=8, cg_rtol=1e-10, cg_check_every=1, conv_norm=M.CONV_B, precision=prec)
+    c.update(kw)
+    return M.HeadSolveConfig(**c)
+
+
+def _fields(M, grids, sigma2=2.0, lam=6.0, seed=100):
+    return [M.generate_K_field(g, sigma2, (lam, lam, lam), seed=seed + r) for r, g in enumerate(grids)]
+
+
+def _single(M, grids, bc, cfg, Ks):
+    import torch
+    out = []
+    for g, K in zip(grids, Ks):
+        s = M.HeadSolver(g, bc, cfg, stream=torch.cuda.current_stream().cuda_stream)
+        s.set_K(K)
+        h = torch.empty_like(K)
+        res = s.solve(h)
+        out.append((h.cpu().numpy(), res))
+        s.close()
+    return out
+
+
+def _batch(M, grids, bc, cfg, Ks, tune=False, x0s=None):
+    import torch
+    b = M.BatchSolver(grids, bc, cfg, stream=torch.cuda.current_stream().cuda_stream)
+    b.set_K(Ks)
+    tuning = b.autotune(2) if tune else None
+    hs = [torch.full_like(K, float("nan")) for K in Ks]
+    res = b.solve(hs, x0s)
+    torch.cuda.synchronize()
+    out = [(h.cpu().numpy(), r) for h, r in zip(hs, res)]
+    return b, out, tuning
+
+
+def _rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64", "bf16"])
+def test_batch_matches_single_solves(mf3d, prec):
+    M = mf3d
+    P = {"fp32": M.PREC_FP32, "fp64": M.PREC_FP64, "bf16": M.PREC_BF16}[prec]
+    grids = _grids(M)
+    bc = M.BCSpec.darcy_x()
+    cfg = _cfg(M, P)
+    Ks = _fields(M, grids)
+    ref = _single(M, grids, bc, cfg, Ks)
+    b, got, _ = _batch(M, grids, bc, cfg, Ks)
+    for (hr, rr), (hb, rb) in zip(ref, got):
+        assert rr.converged and rb.converged, (rr, rb)
+        assert np.all(np.isfinite(hb))
+        assert abs(rb.num_iterations - rr.num_iterations) <= ITER_SLACK[prec], (rb.num_iterations, rr.num_iterations)
+        assert rb.true_rel_residual <= 1e-10
+        assert rb.num_levels == rr.num_levels
+        assert _rel(hb, hr) < HEAD_TOL
+    b.close()
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_batch_iterates_match_single_solves(mf3d, prec):
+    """Six iterations, no convergence: the batched and the single iterates agree to rounding."""
+    M = mf3d
+    P = {"fp32": M.PREC_FP32, "fp64": M.PREC_FP64}[prec]
+    grids = _grids(M)
+    bc = M.BCSpec.darcy_x()
+    cfg = _cfg(M, P, cg_max_iter=6)
+    Ks = _fields(M, grids, seed=200)
+    ref = _single(M, grids, bc, cfg, Ks)
+    b, got, _ = _batch(M, grids, bc, cfg, Ks)
+    for (hr, rr), (hb, rb) in zip(ref, got):
+        assert rr.num_iterations == rb.num_iterations == 6 and not rb.converged
+        assert _rel(hb, hr) < ITERATE_TOL
+        assert abs(rb.final_residual - rr.final_residual) <= 1e-6 * rr.final_residual
+    b.close()
+
+
+def test_convergence_mask_freezes_finished_realisations(mf3d):
+    """A homogeneous K converges in a few iterations, a sigma^2 = 4 field in many more; the
+    easy realisation must report its own count and keep its own converged head."""
+    import torch
+    M = mf3d
+    grids = [M.Grid3D(32, 32, 32, 1.0), M.Grid3D(48, 32, 32, 1.0), M.Grid3D(32, 48, 64, 1.0)]
+    bc = M.BCSpec.darcy_x()
+    cfg = _cfg(M, M.PREC_FP32)
+    Ks = [torch.ones((32, 32, 32), dtype=torch.float64, device="cuda"),
+          M.generate_K_field(grids[1], 4.0, (8.0, 8.0, 8.0), seed=5),
+          M.generate_K_field(grids[2], 1.0, (4.0, 4.0, 4.0), seed=6)]
+    ref = _single(M, grids, bc, cfg, Ks)
+    its = [r.num_iterations for _, r in ref]
+    assert its[0] < its[1] - 3, its
+    b, got, _ = _batch(M, grids, bc, cfg, Ks)
+    for (hr, rr), (hb, rb) in zip(ref, got):
+        assert rb.converged and abs(rb.num_iterations - rr.num_iterations) <= 1
+        assert _rel(hb, hr) < HEAD_TOL
+    b.close()
+
+
+def test_autotune_keeps_results(mf3d):
+    M = mf3d
+    grids = _grids(M)
+    bc = M.BCSpec.darcy_x()
+    cfg = _cfg(M, M.PREC_FP32)
+    Ks = _fields(M, grids, seed=300)
+    b0, base, _ = _batch(M, grids, bc, cfg, Ks)
+    b1, tuned, tuning = _batch(M, grids, bc, cfg, Ks, tune=True)
+    assert tuning and all(t["ms_best"] <= t["ms_default"] + 1e-9 for t in tuning)
+    assert {t["path"] for t in tuning} <= {0, 1}
+    for (h0, r0), (h1, r1) in zip(base, tuned):
+        assert r1.converged and abs(r1.num_iterations - r0.num_iterations) <= 1
+        assert _rel(h1, h0) < HEAD_TOL
+    # solving again after tuning repeats the tuned result exactly (deterministic reductions)
+    import torch
+    hs = [torch.empty_like(K) for K in Ks]
+    res = b1.solve(hs)
+    torch.cuda.synchronize()
+    for h, (h1, r1), r in zip(hs, tuned, res):
+        assert r.num_iterations == r1.num_iterations
+        assert np.array_equal(h.cpu().numpy(), h1)
+    b0.close()
+    b1.close()
+
+
+def test_host_loop_equals_graph(mf3d):
+    M = mf3d
+    grids = _grids(M)[:3]
+    bc = M.BCSpec.darcy_x()
+    Ks = _fields(M, grids, seed=400)
+    bg, g, _ = _batch(M, grids, bc, _cfg(M, M.PREC_FP32), Ks)
+    bh, h, _ = _batch(M, grids, bc, _cfg(M, M.PREC_FP32, use_graph=0), Ks)
+    for (ha, ra), (hb, rb) in zip(g, h):
+        assert ra.num_iterations == rb.num_iterations
+        assert np.array_equal(ha, hb)
+    bg.close()
+    bh.close()
+
+
+def test_warm_start_and_iteration_cap(mf3d):
+    """x0 per realisation (None entries use the reference guess); a cap of 3 iterations stops
+    every realisation unconverged with 3 iterations."""
+    import torch
+    M = mf3d
+    grids = _grids(M)[:3]
+    bc = M.BCSpec.darcy_x()
+    Ks = _fields(M, grids, seed=500)
+    b, got, _ = _batch(M, grids, bc, _cfg(M, M.PREC_FP32), Ks)
+    x0s = [torch.from_numpy(got[0][0]).cuda(), None, torch.from_numpy(got[2][0]).cuda()]
+    hs = [torch.empty_like(K) for K in Ks]
+    res = b.solve(hs, x0s)
+    assert res[0].num_iterations <= 1 and res[2].num_iterations <= 1
+    assert res[1].num_iterations == got[1][1].num_iterations
+    b.close()
+    bcap, capped, _ = _batch(M, grids, bc, _cfg(M, M.PREC_FP32, cg_max_iter=3), Ks)
+    for _, r in capped:
+        assert r.num_iterations == 3 and not r.converged
+    bcap.close()
+
+
+def test_nonfinite_realisation_does_not_stop_the_others(mf3d):
+    import torch
+    M = mf3d
+    grids = _grids(M)[:3]
+    bc = M.BCSpec.darcy_x()
+    cfg = _cfg(M, M.PREC_FP32)
+    Ks = _fields(M, grids, seed=600)
+    Ks[1] = Ks[1].clone()
+    Ks[1].view(-1)[17] = float("nan")
+    ref = _single(M, [grids[0], grids[2]], bc, cfg, [Ks[0], Ks[2]])
+    b, got, _ = _batch(M, grids, bc, cfg, Ks)
+    assert got[1][1].status == 2 and not got[1][1].converged
+    for (hr, rr), (hb, rb) in zip(ref, [got[0], got[2]]):
+        assert rb.converged and abs(rb.num_iterations - rr.num_iterations) <= 1
+        assert _rel(hb, hr) < HEAD_TOL
+    b.close()

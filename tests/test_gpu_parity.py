@@ -93,11 +93,15 @@ def test_transfer_vs_oracle(mf3d, oracle_mod):
 
 @pytest.mark.parametrize("shape,levels,pre,post,coarse", [
     ((16, 16, 16), 3, 2, 2, 50), ((32, 32, 32), 4, 2, 2, 50), ((64, 32, 32), 4, 1, 3, 20),
-    ((8, 8, 8), 2, 2, 2, 50), ((64, 64, 64), 5, 2, 2, 50)])
+    ((8, 8, 8), 2, 2, 2, 50), ((64, 64, 64), 5, 2, 2, 50),
+    # level 1 is 18 / 26 cells wide: 16-byte rows in FP64 but not whole 4-cell quads
+    ((16, 20, 36), 3, 2, 2, 50), ((24, 16, 52), 3, 2, 2, 20)])
 @pytest.mark.parametrize("case", BC_CASES[:4], ids=[c[0] for c in BC_CASES[:4]])
 def test_vcycle_vs_oracle(mf3d, oracle_mod, shape, levels, pre, post, coarse, case):
     M, O = mf3d, oracle_mod
     name, types, values, pin = case
+    if types[0] == P and (shape[2] >> (levels - 1)) % 2:
+        pytest.skip("periodic x with an odd count on the coarsest level: red-black order is undefined")
     rng = np.random.default_rng(zlib.crc32(repr((shape, name, 1)).encode()))
     K = np.exp(rng.normal(size=shape))
     r = rng.normal(size=shape)
