@@ -194,6 +194,118 @@ def e2e_steps(M, n, K_host, precision, steps, warmup):
     return steps / (ms / 1e3), nbytes, nbytes
 
 
+ENSEMBLE_EDGES = (64, 96, 128, 160)
+
+
+def ensemble_shapes(seed, count):
+    """Grid edges drawn uniformly from ENSEMBLE_EDGES per axis and realisation (uneven sizes)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return [tuple(int(e) for e in rng.choice(ENSEMBLE_EDGES, 3)) for _ in range(count)]
+
+
+def ensemble_steps(M, prec, count, steps, warmup, seed, tune_reps=3):
+    """Monte Carlo ensemble: `count` realisations of uneven grids (sigma^2 = 2, lambda = 6, seed
+    + r), each step = set-up from K + PCG to ||r||/||b|| <= 1e-10 + face velocity for every
+    realisation.  Batched (mf3d_batch_*: one graph for all) against looping single solves
+    (one HeadSolver per distinct grid, reused as FlowWorkspace is)."""
+    import torch
+    shapes = ensemble_shapes(seed, count)
+    grids = [M.Grid3D(nx, ny, nz, 1.0) for nx, ny, nz in shapes]
+    lv = min(levels_for(e) for sh in shapes for e in sh)
+    cfg = M.HeadSolveConfig(mg_levels=max(lv, 6), mg_pre_smooth=2, mg_post_smooth=2, mg_coarse_iters=50,
+                            cg_max_iter=500, cg_check_every=1, cg_rtol=1e-10, conv_norm=M.CONV_B,
+                            precision=prec, use_graph=USE_GRAPH)
+    bc = M.BCSpec.darcy_x()
+    stream = torch.cuda.current_stream()
+    Ks = [M.generate_K_field(g, 2.0, (6.0, 6.0, 6.0), seed=seed + r, n_modes=1000) for r, g in enumerate(grids)]
+    hs = [torch.empty_like(K) for K in Ks]
+    vel = [[torch.empty(q, dtype=torch.float64, device="cuda") for q in M.velocity_sizes(g)] for g in grids]
+    cells = sum(g.num_cells() for g in grids)
+
+    def velocities():
+        for g, h, K, (U, V, W) in zip(grids, hs, Ks, vel):
+            M.compute_velocity_from_head(U, V, W, h, K, g, bc)
+
+    def timed(step):
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = None
+        for _ in range(steps):
+            out = step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), out
+
+    # ---- batched ----
+    b = M.BatchSolver(grids, bc, cfg, stream=stream.cuda_stream)
+    solvers = {}
+    try:
+        return _ensemble_arms(M, b, solvers, grids, shapes, bc, cfg, Ks, hs, velocities, timed, cells, count,
+                              steps, warmup, tune_reps)
+    finally:
+        torch.cuda.synchronize()
+        b.close()
+        for s in solvers.values():
+            s.close()
+
+
+def _ensemble_arms(M, b, solvers, grids, shapes, bc, cfg, Ks, hs, velocities, timed, cells, count, steps, warmup,
+                   tune_reps):
+    import torch
+    stream = torch.cuda.current_stream()
+    b.set_K(Ks)
+    tuning = b.autotune(tune_reps) if tune_reps > 0 else []
+
+    def bstep():
+        b.set_K(Ks)
+        r = b.solve(hs)
+        velocities()
+        return r
+
+    ms_b, res_b = timed(bstep)
+    h_batch = [h.clone() for h in hs[:4]]
+    # ---- looping single solves ----
+    for g, sh in zip(grids, shapes):
+        if sh not in solvers:
+            solvers[sh] = M.HeadSolver(g, bc, cfg, stream=stream.cuda_stream)
+
+    def lstep():
+        out = []
+        for sh, K, h in zip(shapes, Ks, hs):
+            s = solvers[sh]
+            s.set_K(K)
+            out.append(s.solve(h))
+        velocities()
+        return out
+
+    ms_l, res_l = timed(lstep)
+    dh = max(((a - h).abs().max() / h.abs().max()).item() for a, h in zip(h_batch, hs[:4]))
+    its_b = [r.num_iterations for r in res_b]
+    its_l = [r.num_iterations for r in res_l]
+    out = {"workload": f"{count} realisations, edges from {{{','.join(map(str, ENSEMBLE_EDGES))}}} per axis, "
+                       "sigma2 2, lambda 6, seed + r, FP32 V-cycle in flexible FP64 PCG to ||r||/||b|| <= 1e-10",
+           "cells_total": cells, "distinct_grids": len(solvers),
+           "step": "set-up from K + PCG + face velocity, every realisation",
+           "batched_solves_per_s": round(count * steps / (ms_b / 1e3), 3),
+           "looped_solves_per_s": round(count * steps / (ms_l / 1e3), 3),
+           "speedup_batched_vs_looped": round(ms_l / ms_b, 3),
+           "batched_cell_solves_per_s": round(cells * steps / (ms_b / 1e3), 1),
+           "batched_ms_per_step": round(ms_b / steps, 3), "looped_ms_per_step": round(ms_l / steps, 3),
+           "iterations_batched": [min(its_b), max(its_b)], "iterations_looped": [min(its_l), max(its_l)],
+           "all_converged": bool(all(r.converged for r in res_b) and all(r.converged for r in res_l)),
+           "max_true_rel_residual": max(r.true_rel_residual for r in res_b),
+           "head_rel_maxdiff_batched_vs_looped": dh,
+           "batched_launches_per_step": res_b[0].kernel_launches,
+           "autotune_positions": len(tuning),
+           "autotune_gain_ms": round(sum(t["ms_default"] - t["ms_best"] for t in tuning), 4),
+           "steps": steps, "warmup": warmup, "device_bytes_batched": b.device_bytes}
+    return out
+
+
 def cpu_baseline(K_np, n, iters_needed, budget_s=20.0):
     """The oracle (OpenMP restatement of the reference CCMG-PCG) on all host cores, on a
     bounded sample: set-up + 1 and + 3 PCG iterations of the same solve, extrapolated to the
@@ -260,6 +372,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--profile-kernels", action="store_true", help="print per-kernel timings")
     ap.add_argument("--seed", type=int, default=20240601)
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched Monte Carlo ensemble")
+    ap.add_argument("--ensemble-only", action="store_true",
+                    help="run only the batched Monte Carlo ensemble and print its record")
+    ap.add_argument("--ensemble-count", type=int, default=128)
     ap.add_argument("--no-graph", action="store_true",
                     help="host-driven PCG loop instead of the CUDA-graph while loop (for profilers)")
     args = ap.parse_args()
@@ -304,6 +420,17 @@ def main():
     from macroflow3d_b200 import build
     build.build_lib()
     prec = {"fp64": M.PREC_FP64, "fp32": M.PREC_FP32, "bf16": M.PREC_BF16}[args.precision]
+    if args.ensemble_only:
+        if rank == 0:
+            with Clocks(torch.cuda.current_device()) as clk:
+                ens = ensemble_steps(M, prec, args.ensemble_count, args.steps, args.warmup, args.seed)
+            ens["clocks"] = clk.summary()
+            print(json.dumps({"metric": "ensemble_solves_per_s", "value": ens["batched_solves_per_s"],
+                              "unit": "solves/s", "ensemble": ens}), flush=True)
+        if dist_ctx is not None:
+            dist_ctx.barrier()
+            dist_ctx.destroy_process_group()
+        return
     K = make_K(M, n, sigma2, lam, args.seed + rank, torch.cuda.current_device())
     torch.cuda.synchronize()
 
@@ -357,6 +484,10 @@ def main():
                        "d2h_bytes_per_step": bo}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(K.cpu().numpy(), n, iters64)
+    if rank == 0 and world == 1 and not args.no_ensemble:
+        del K
+        torch.cuda.empty_cache()
+        line["ensemble"] = ensemble_steps(M, prec, args.ensemble_count, 3, 3, args.seed)
 
     if rank == 0:
         print(json.dumps(line), flush=True)

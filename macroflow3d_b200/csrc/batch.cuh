@@ -167,9 +167,9 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
             Blob b;
             b.add(items.data(), items.size() * sizeof(items[0]));
             tail_mem_ = b.upload();
-            if (tail_smem_ > 48 * 1024)
-                MF3D_CK(cudaFuncSetAttribute(tail2_batch_kernel<T, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)tail_smem_));
+            // largest tail of any batch (the attribute is the kernel's, shared by all batches)
+            MF3D_CK(cudaFuncSetAttribute(tail2_batch_kernel<T, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTailSmemMax));
         }
         // ---- PCG items and the launch tables of the cell and streaming kernels ----
         {

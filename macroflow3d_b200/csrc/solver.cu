@@ -35,6 +35,9 @@ namespace mf3d {
 
 static thread_local std::string g_err;
 
+// Shared memory of the one-CTA coarse tail (padded x and b of its levels), at most.
+static constexpr size_t kTailSmemMax = 200 * 1024;
+
 // Device-time limit of one solve: the PCG loop stops with status 3 after this long.
 static constexpr unsigned long long kSolveBudgetNs = 120ull * 1000000000ull;
 
@@ -432,12 +435,14 @@ template <class T, class TC> class VCycle : public VCycleBase {
             tail_smem_ = (size_t)off * sizeof(double);
             tail_out_.reset(new DevMem(G[Lt].n * sizeof(T)));
             bytes_ += G[Lt].n * sizeof(T);
-            if (tail_smem_ > 48 * 1024) {
-                MF3D_CK(cudaFuncSetAttribute(tail2_kernel<T, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)tail_smem_));
-                MF3D_CK(cudaFuncSetAttribute(tail2_kernel<double, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)tail_smem_));
-            }
+            // the attribute belongs to the kernel, not to this solver: set it to the largest
+            // tail any solver may have, so that a solver created later with a smaller tail does
+            // not lower it under this one
+            if (tail_smem_ > kTailSmemMax) throw Error(MF3D_E_INVALID, "coarse tail exceeds shared memory");
+            MF3D_CK(cudaFuncSetAttribute(tail2_kernel<T, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTailSmemMax));
+            MF3D_CK(cudaFuncSetAttribute(tail2_kernel<double, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTailSmemMax));
         }
     }
 
@@ -857,11 +862,11 @@ class HeadSolver {
         };
         Lt_ = nl - 1;
         size_t tbytes = tail_bytes(nl - 1);
-        while (Lt_ > 0 && G_[Lt_ - 1].n <= 4096 && tbytes + tail_bytes(Lt_ - 1) <= 200 * 1024) {
+        while (Lt_ > 0 && G_[Lt_ - 1].n <= 4096 && tbytes + tail_bytes(Lt_ - 1) <= kTailSmemMax) {
             --Lt_;
             tbytes += tail_bytes(Lt_);
         }
-        if (tbytes > 200 * 1024)
+        if (tbytes > kTailSmemMax)
             throw Error(MF3D_E_INVALID, "coarsest level too large for the coarse solver (raise mg_levels)");
         if (user_stream) {
             stream_ = user_stream;

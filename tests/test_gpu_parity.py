@@ -161,6 +161,21 @@ def test_mixed_precision_reaches_fp64_tolerance(mf3d, oracle_mod, prec):
     assert _rel(_np(h), ho) < 1e-7
 
 
+def test_solvers_with_different_coarse_tails_coexist(mf3d):
+    """A solver created later with a smaller coarse tail must not lower the tail kernel's
+    shared-memory limit under an earlier solver's tail."""
+    M = mf3d
+    g = M.Grid3D(32, 32, 32, 1.0)
+    K = _t(_lognormal((32, 32, 32), 1.0, 21))
+    cfg = dict(cg_rtol=1e-10, cg_check_every=1, conv_norm=M.CONV_B)
+    big = M.HeadSolver(g, M.BCSpec.darcy_x(), M.HeadSolveConfig(mg_levels=5, **cfg))
+    small = M.HeadSolver(g, M.BCSpec.darcy_x(), M.HeadSolveConfig(mg_levels=2, **cfg))
+    for s in (big, small, big):
+        s.set_K(K)
+        h = _t(np.zeros((32, 32, 32)))
+        assert s.solve(h).converged
+
+
 def test_graph_and_host_loop_identical(mf3d):
     M = mf3d
     shape = (32, 32, 32)
