@@ -220,6 +220,45 @@ int mf3d_batch_solve(mf3d_batch* b, double* const* h_dev, const double* const* x
  * records and sets *count.  The solver state is scratch afterwards (the next solve rebuilds it). */
 int mf3d_batch_autotune(mf3d_batch* b, int reps, mf3d_batch_tuning* out, int cap, int* count);
 
+/* ---- learned warm start (no counterpart in the reference, whose initial guess is the
+ * x-linear head, src/physics/flow/solve_head.cu:29-73) ----------------------------------------
+ * A 3-D convolutional encoder-decoder (4 levels, 16/32/64/64 channels, 3x3x3 convolutions, skip
+ * connections; BF16 weights and activations, FP32 accumulation on the tensor cores) maps lnK
+ * and the x-linear head to a correction of that head; x0 = h_lin + correction is passed to
+ * mf3d_head_solve as its initial guess, which still iterates to its tolerance.  Trained with
+ * this library's forward and backward kernels and Adam on (lnK, head) pairs from the solver.
+ * Grid sizes must be multiples of 8 on every axis. */
+typedef struct mf3d_warmstart mf3d_warmstart;
+int mf3d_ws_create(unsigned long long seed, mf3d_warmstart** out);
+int mf3d_ws_destroy(mf3d_warmstart* w);
+long long mf3d_ws_num_params(const mf3d_warmstart* w);
+/* FP32 master parameters, per layer the weights [cout][27][cin] then the bias [cout] */
+int mf3d_ws_get_params(const mf3d_warmstart* w, float* host);
+int mf3d_ws_set_params(mf3d_warmstart* w, const float* host);
+/* gradient of the last mf3d_ws_train_step, summed over its samples (same layout) */
+int mf3d_ws_get_grads(const mf3d_warmstart* w, float* host);
+/* One Adam step on `count` samples (lnK_dev[i], h_dev[i]: FP32 device arrays of grid g) with
+ * the mean gradient of the mean squared error of the predicted head; lr <= 0 computes the
+ * gradients only.  *loss: mean loss before the step. */
+int mf3d_ws_train_step(mf3d_warmstart* w, const mf3d_grid* g, const mf3d_bc* bc, int count,
+                       const float* const* lnK_dev, const float* const* h_dev, float lr, double* loss,
+                       void* stream);
+int mf3d_ws_eval(mf3d_warmstart* w, const mf3d_grid* g, const mf3d_bc* bc, int count,
+                 const float* const* lnK_dev, const float* const* h_dev, double* loss, void* stream);
+/* x0_dev (FP64, n) = x-linear head of bc's x faces + the network's correction, from K_dev (FP64) */
+int mf3d_ws_predict(mf3d_warmstart* w, const mf3d_grid* g, const mf3d_bc* bc, const double* K_dev,
+                    double* x0_dev, void* stream);
+/* The network's operations, for tests: a 3x3x3 convolution on the tensor cores (x: BF16
+ * [n][cin], w: BF16 [cout][27][cin], bias FP32 or NULL, relu 0/1, mask BF16 [n][cout] or NULL:
+ * y *= (mask > 0), y: BF16 or (y_f32) FP32 [n][cout]; channels multiples of 16 up to 128), the
+ * weight flip that turns the data gradient into a convolution, and the weight gradient
+ * (dw FP32 [cout][27][cin], db FP32 [cout]). */
+int mf3d_nn_conv3d(const mf3d_grid* g, int cin, int cout, const void* x_dev, const void* w_dev,
+                   const float* bias_dev, int relu, const void* mask_dev, int y_f32, void* y_dev, void* stream);
+int mf3d_nn_flip_weights(int cin, int cout, const void* w_dev, void* wt_dev, void* stream);
+int mf3d_nn_conv3d_wgrad(const mf3d_grid* g, int cin, int cout, const void* x_dev, const void* dy_dev,
+                         float* dw_dev, float* db_dev, void* stream);
+
 /* ---- operator pieces (device pointers, FP64; in-place where the reference is) ------------- */
 /* VarCoeffLaplacian::apply, src/numerics/operators/varcoeff_laplacian.cu:241-277 */
 int mf3d_apply_A(const mf3d_grid* g, const mf3d_bc* bc, int pin, const double* K, const double* x,

@@ -255,6 +255,128 @@ class BatchSolver:
                      ms_default=t.ms_default, ms_best=t.ms_best) for t in arr[:cnt.value]]
 
 
+class WarmStart:
+    """Learned PCG initial guess (no counterpart in the reference, whose guess is the x-linear
+    head, src/physics/flow/solve_head.cu:29-73): a 3-D convolutional encoder-decoder on the
+    tensor cores, trained with this library's own forward and backward kernels on lnK -> head
+    pairs that the solver generates.  predict() writes x0 = h_lin + net(lnK) for
+    HeadSolver.solve(h, x0); PCG still runs to its tolerance, so the network changes only the
+    iteration count and the time."""
+
+    def __init__(self, seed: int = 0):
+        h = C.c_void_p()
+        check(lib().mf3d_ws_create(int(seed), C.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().mf3d_ws_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def num_params(self) -> int:
+        return int(lib().mf3d_ws_num_params(self._h))
+
+    def get_params(self):
+        import numpy as np
+        p = np.empty(self.num_params, dtype=np.float32)
+        check(lib().mf3d_ws_get_params(self._h, p.ctypes.data))
+        return p
+
+    def set_params(self, p) -> None:
+        import numpy as np
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.size != self.num_params:
+            raise ValueError(f"expected {self.num_params} parameters, got {p.size}")
+        check(lib().mf3d_ws_set_params(self._h, p.ctypes.data))
+
+    def get_grads(self):
+        import numpy as np
+        g = np.empty(self.num_params, dtype=np.float32)
+        check(lib().mf3d_ws_get_grads(self._h, g.ctypes.data))
+        return g
+
+    def save(self, path: str) -> None:
+        import numpy as np
+        np.save(path, self.get_params())
+
+    def load(self, path: str) -> None:
+        import numpy as np
+        self.set_params(np.load(path))
+
+    @staticmethod
+    def _f32_ptrs(arrays, n, what):
+        import torch
+        out = (C.c_void_p * len(arrays))()
+        for i, a in enumerate(arrays):
+            if a.dtype != torch.float32 or not a.is_cuda or not a.is_contiguous() or a.numel() != n:
+                raise ValueError(f"{what}[{i}] must be a contiguous float32 CUDA tensor of {n} cells")
+            out[i] = a.data_ptr()
+        return out
+
+    def train_step(self, grid: Grid3D, bc: BCSpec, lnKs, hs, lr: float) -> float:
+        """One Adam step on the mean gradient of the samples (lnK, h: float32 CUDA tensors);
+        lr = 0 computes the gradients only (get_grads).  Returns the mean loss."""
+        n = grid.num_cells()
+        loss = C.c_double(0.0)
+        check(lib().mf3d_ws_train_step(self._h, C.byref(grid.c()), C.byref(_bc(bc)), len(lnKs),
+                                       self._f32_ptrs(lnKs, n, "lnK"), self._f32_ptrs(hs, n, "h"), float(lr),
+                                       C.byref(loss), _stream()))
+        return loss.value
+
+    def eval(self, grid: Grid3D, bc: BCSpec, lnKs, hs) -> float:
+        n = grid.num_cells()
+        loss = C.c_double(0.0)
+        check(lib().mf3d_ws_eval(self._h, C.byref(grid.c()), C.byref(_bc(bc)), len(lnKs),
+                                 self._f32_ptrs(lnKs, n, "lnK"), self._f32_ptrs(hs, n, "h"), C.byref(loss),
+                                 _stream()))
+        return loss.value
+
+    def predict(self, grid: Grid3D, bc: BCSpec, K, x0) -> None:
+        """x0 (float64 CUDA) = the x-linear head + the network's correction, from K (float64 CUDA)."""
+        n = grid.num_cells()
+        check(lib().mf3d_ws_predict(self._h, C.byref(grid.c()), C.byref(_bc(bc)), _f64(K, n, "K"),
+                                    _f64(x0, n, "x0"), _stream()))
+
+
+def nn_conv3d(grid: Grid3D, x, w, bias=None, relu=False, mask=None, out_f32=False):
+    """One tensor-core 3x3x3 convolution (BF16 x [V, cin], w [cout, 27, cin]; FP32 bias [cout])."""
+    import torch
+    cin, cout = w.shape[2], w.shape[0]
+    y = torch.empty((grid.num_cells(), cout), dtype=torch.float32 if out_f32 else torch.bfloat16, device=x.device)
+    check(lib().mf3d_nn_conv3d(C.byref(grid.c()), int(cin), int(cout), x.data_ptr(), w.data_ptr(),
+                               None if bias is None else bias.data_ptr(), int(bool(relu)),
+                               None if mask is None else mask.data_ptr(), int(bool(out_f32)), y.data_ptr(),
+                               _stream()))
+    return y
+
+
+def nn_flip_weights(w):
+    """W'[ci, t, co] = W[co, 26 - t, ci] (BF16): the data gradient as a forward convolution."""
+    import torch
+    cout, _, cin = w.shape
+    wt = torch.empty((cin, 27, cout), dtype=torch.bfloat16, device=w.device)
+    check(lib().mf3d_nn_flip_weights(int(cin), int(cout), w.data_ptr(), wt.data_ptr(), _stream()))
+    return wt
+
+
+def nn_conv3d_wgrad(grid: Grid3D, x, dy):
+    """(dW [cout, 27, cin], db [cout]) in FP32 from BF16 x [V, cin] and dy [V, cout]."""
+    import torch
+    cin, cout = x.shape[1], dy.shape[1]
+    dw = torch.empty((cout, 27, cin), dtype=torch.float32, device=x.device)
+    db = torch.empty((cout,), dtype=torch.float32, device=x.device)
+    check(lib().mf3d_nn_conv3d_wgrad(C.byref(grid.c()), int(cin), int(cout), x.data_ptr(), dy.data_ptr(),
+                                     dw.data_ptr(), db.data_ptr(), _stream()))
+    return dw, db
+
+
 def solve_head(h, K, grid: Grid3D, bc: BCSpec, cfg: HeadSolveConfig,
                workspace: Optional[HeadSolver] = None) -> Tuple[HeadSolveResult, HeadSolver]:
     """solve_head (src/physics/flow/solve_head.cuh:158-160).  Returns (result, workspace);

@@ -74,6 +74,19 @@ SIGNATURES = {
     "mf3d_batch_set_K": ([_P, C.POINTER(_P)], C.c_int),
     "mf3d_batch_solve": ([_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(SolveResult)], C.c_int),
     "mf3d_batch_autotune": ([_P, C.c_int, C.POINTER(BatchTuning), C.c_int, C.POINTER(C.c_int)], C.c_int),
+    "mf3d_ws_create": ([C.c_ulonglong, C.POINTER(_P)], C.c_int),
+    "mf3d_ws_destroy": ([_P], C.c_int),
+    "mf3d_ws_num_params": ([_P], C.c_longlong),
+    "mf3d_ws_get_params": ([_P, _P], C.c_int),
+    "mf3d_ws_set_params": ([_P, _P], C.c_int),
+    "mf3d_ws_get_grads": ([_P, _P], C.c_int),
+    "mf3d_ws_train_step": ([_P, _G, _B, C.c_int, C.POINTER(_P), C.POINTER(_P), C.c_float,
+                            C.POINTER(C.c_double), _P], C.c_int),
+    "mf3d_ws_eval": ([_P, _G, _B, C.c_int, C.POINTER(_P), C.POINTER(_P), C.POINTER(C.c_double), _P], C.c_int),
+    "mf3d_ws_predict": ([_P, _G, _B, _P, _P, _P], C.c_int),
+    "mf3d_nn_conv3d": ([_G, C.c_int, C.c_int, _P, _P, _P, C.c_int, _P, C.c_int, _P, _P], C.c_int),
+    "mf3d_nn_flip_weights": ([C.c_int, C.c_int, _P, _P, _P], C.c_int),
+    "mf3d_nn_conv3d_wgrad": ([_G, C.c_int, C.c_int, _P, _P, _P, _P, _P], C.c_int),
     "mf3d_velocity_from_head": ([_G, _B, _P, _P, C.c_int, _P, _P, _P, _P], C.c_int),
     "mf3d_velocity_mass_balance": ([_G, _B, _P, _P, _P, _P, _P, C.POINTER(C.c_double), _P], C.c_int),
     "mf3d_velocity_mass_balance_noalloc": ([_G, _B, _P, _P, _P, _P, _P, C.POINTER(C.c_double), _P], C.c_int),

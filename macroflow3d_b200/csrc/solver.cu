@@ -1800,3 +1800,4 @@ int mf3d_kfield_eval(const mf3d_grid* g, int n_modes, const double* modes, doubl
 } // extern "C"
 
 #include "batch.cuh"
+#include "nn.cuh"

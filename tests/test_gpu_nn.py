@@ -1,0 +1,182 @@
+"""The warm-start network's CUDA kernels against the FP64 oracle (oracle/nn_oracle.py).
+
+Inputs and weights are BF16 on both sides (the oracle gets the same rounded values); the
+tensor cores accumulate in FP32, so an FP32 output matches the oracle to ~1e-5 relative and a
+BF16 output to its rounding (2^-8).  The whole-network gradient goes through BF16
+activations and BF16 intermediate gradients, so it is compared by relative norm (a few 1e-3)
+and direction.  Then: training with these kernels lowers the loss, and the trained network's
+initial guess saves PCG iterations on held-out fields.
+"""
+import numpy as np
+import pytest
+
+from oracle import nn_oracle as N
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).cuda().to(torch.bfloat16)
+
+
+def _np(t):
+    import torch
+    return t.float().cpu().numpy().astype(np.float64) if t.dtype == torch.bfloat16 else t.cpu().numpy().astype(np.float64)
+
+
+def _rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+SHAPES = [(8, 8, 8), (5, 6, 10), (16, 8, 12)]  # (nz, ny, nx): full tiles, a ragged last tile
+CHANNELS = [(16, 16), (16, 48), (32, 64), (48, 16), (64, 128), (96, 32), (128, 64)]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("cin,cout", CHANNELS)
+def test_conv3d_forward_vs_oracle(mf3d, shape, cin, cout):
+    import torch
+    M = mf3d
+    r = np.random.default_rng(hash((shape, cin, cout)) % 2 ** 32)
+    nz, ny, nx = shape
+    g = M.Grid3D(nx, ny, nz, 1.0)
+    x = _bf(r.normal(size=(nz * ny * nx, cin)))
+    w = _bf(r.normal(size=(cout, 27, cin)) / np.sqrt(27 * cin))
+    b = torch.from_numpy(r.normal(size=cout).astype(np.float32)).cuda()
+    X = _np(x).reshape(nz, ny, nx, cin)
+    W = _np(w)
+    ref = N.conv3d(X, W, b.cpu().numpy().astype(np.float64)).reshape(-1, cout)
+    y = M.nn_conv3d(g, x, w, b, out_f32=True)
+    assert _rel(_np(y), ref) < 2e-5
+    # ReLU and BF16 output
+    yr = M.nn_conv3d(g, x, w, b, relu=True)
+    np.testing.assert_allclose(_np(yr), np.maximum(ref, 0.0), rtol=1e-2, atol=1e-2 * np.abs(ref).max())
+    # the ReLU-derivative mask of another activation
+    mask = _bf(r.normal(size=(nz * ny * nx, cout)))
+    ym = M.nn_conv3d(g, x, w, None, mask=mask, out_f32=True)
+    refm = N.conv3d(X, W).reshape(-1, cout) * (_np(mask) > 0)
+    assert _rel(_np(ym), refm) < 2e-5
+
+
+@pytest.mark.parametrize("cin,cout", [(16, 16), (48, 16), (128, 64), (96, 32)])
+def test_conv3d_data_gradient_vs_oracle(mf3d, cin, cout):
+    M = mf3d
+    r = np.random.default_rng(cin * 1000 + cout)
+    nz, ny, nx = 6, 8, 12
+    g = M.Grid3D(nx, ny, nz, 1.0)
+    w = _bf(r.normal(size=(cout, 27, cin)) / np.sqrt(27 * cin))
+    dy = _bf(r.normal(size=(nz * ny * nx, cout)))
+    wt = M.nn_flip_weights(w)
+    np.testing.assert_array_equal(_np(wt), N.flip_weights(_np(w)))
+    dx = M.nn_conv3d(g, dy, wt, out_f32=True)
+    ref = N.conv3d_dgrad(_np(dy).reshape(nz, ny, nx, cout), _np(w)).reshape(-1, cin)
+    assert _rel(_np(dx), ref) < 2e-5
+
+
+@pytest.mark.parametrize("cin,cout", [(16, 16), (16, 32), (48, 16), (128, 64)])
+def test_conv3d_weight_gradient_vs_oracle(mf3d, cin, cout):
+    M = mf3d
+    r = np.random.default_rng(cin * 7 + cout)
+    nz, ny, nx = 8, 10, 12
+    g = M.Grid3D(nx, ny, nz, 1.0)
+    x = _bf(r.normal(size=(nz * ny * nx, cin)))
+    dy = _bf(r.normal(size=(nz * ny * nx, cout)))
+    dw, db = M.nn_conv3d_wgrad(g, x, dy)
+    rw, rb = N.conv3d_wgrad(_np(x).reshape(nz, ny, nx, cin), _np(dy).reshape(nz, ny, nx, cout))
+    assert _rel(_np(dw), rw) < 1e-5
+    assert _rel(_np(db), rb) < 1e-5
+
+
+def _sample(M, n, seed, sigma2=1.0, lam=4.0):
+    """(lnK, h) of one solver-generated pair on an n^3 grid, FP32 CUDA tensors."""
+    import torch
+    g = M.Grid3D(n, n, n, 1.0)
+    lnK = M.generate_K_field(g, sigma2, (lam, lam, lam), seed=seed, log_only=True)
+    K = torch.exp(lnK)
+    cfg = M.HeadSolveConfig(mg_levels=8, cg_rtol=1e-10, cg_check_every=1, conv_norm=M.CONV_B,
+                            precision=M.PREC_FP32)
+    s = M.HeadSolver(g, M.BCSpec.darcy_x(), cfg, stream=torch.cuda.current_stream().cuda_stream)
+    s.set_K(K)
+    h = torch.empty_like(K)
+    res = s.solve(h)
+    s.close()
+    return lnK.float().contiguous(), h.float().contiguous(), K, res
+
+
+def test_network_gradient_vs_oracle(mf3d):
+    import torch
+    M = mf3d
+    n = 16
+    g = M.Grid3D(n, n, n, 1.0)
+    bc = M.BCSpec.darcy_x()
+    lnK, h, _, _ = _sample(M, n, 11)
+    ws = M.WarmStart(seed=5)
+    p = ws.get_params()
+    r = np.random.default_rng(0)
+    p = (p + 0.02 * r.normal(size=p.size) * (np.abs(p) > 0)).astype(np.float32)  # a non-trivial output layer
+    ws.set_params(p)
+    loss = ws.train_step(g, bc, [lnK], [h], 0.0)
+    grad = ws.get_grads().astype(np.float64)
+    # the oracle on the same BF16-rounded weights and the same FP32 inputs
+    pb = torch.from_numpy(p).to(torch.bfloat16).float().numpy().astype(np.float64)
+    sizes = [ci * co * 27 + co for ci, co, _ in N.LAYERS]
+    o = 0
+    for ci, co, _ in N.LAYERS:  # biases stay FP32 on the device
+        pb[o + ci * co * 27:o + ci * co * 27 + co] = p[o + ci * co * 27:o + ci * co * 27 + co]
+        o += ci * co * 27 + co
+    lk = _np(lnK).reshape(n, n, n)
+    hh = _np(h).reshape(n, n, n)
+    lk_b = torch.from_numpy((0.5 * lk).astype(np.float32)).to(torch.bfloat16).float().numpy().astype(np.float64) * 2
+    rl, rg = N.loss_and_grad(pb, lk_b, hh)
+    assert abs(loss - rl) <= 2e-2 * rl, (loss, rl)
+    cos = float(grad @ rg / (np.linalg.norm(grad) * np.linalg.norm(rg)))
+    rel = float(np.linalg.norm(grad - rg) / np.linalg.norm(rg))
+    assert cos > 0.999 and rel < 0.05, (cos, rel)
+    # every layer's gradient, not just the largest ones
+    o = 0
+    for k, (ci, co, _) in enumerate(N.LAYERS):
+        sl = slice(o, o + ci * co * 27 + co)
+        o += ci * co * 27 + co
+        a, b = grad[sl], rg[sl]
+        assert np.linalg.norm(a - b) <= 0.1 * np.linalg.norm(b) + 1e-12, (k, np.linalg.norm(a - b), np.linalg.norm(b))
+    ws.close()
+
+
+def test_training_lowers_the_loss_and_the_guess_saves_iterations(mf3d):
+    import torch
+    M = mf3d
+    n = 32
+    g = M.Grid3D(n, n, n, 1.0)
+    bc = M.BCSpec.darcy_x()
+    data = [_sample(M, n, 100 + i) for i in range(8)]
+    held = _sample(M, n, 999)
+    ws = M.WarmStart(seed=1)
+    lnKs = [d[0] for d in data]
+    hs = [d[1] for d in data]
+    l0 = ws.eval(g, bc, lnKs, hs)
+    for it in range(150):
+        k = 4 * (it % 2)
+        ws.train_step(g, bc, lnKs[k:k + 4], hs[k:k + 4], 1e-3)
+    l1 = ws.eval(g, bc, lnKs, hs)
+    assert l1 < 0.5 * l0, (l0, l1)
+    # held-out field: the predicted guess is closer to the head than the x-linear guess
+    lnK, h, K, res0 = held
+    x0 = torch.empty_like(K)
+    ws.predict(g, bc, K, x0)
+    hl = torch.from_numpy(np.broadcast_to(1.0 - (np.arange(n) + 0.5) / n, (n, n, n)).copy()).cuda().reshape(-1)
+    e_lin = float((hl - h.double().reshape(-1)).norm())
+    e_net = float((x0.reshape(-1) - h.double().reshape(-1)).norm())
+    assert e_net < e_lin, (e_net, e_lin)
+    # PCG from the predicted guess reaches the same tolerance in no more iterations
+    cfg = M.HeadSolveConfig(mg_levels=8, cg_rtol=1e-10, cg_check_every=1, conv_norm=M.CONV_B,
+                            precision=M.PREC_FP32)
+    s = M.HeadSolver(g, bc, cfg, stream=torch.cuda.current_stream().cuda_stream)
+    s.set_K(K)
+    hw = torch.empty_like(K)
+    res = s.solve(hw, x0)
+    assert res.converged and res.true_rel_residual <= 1e-10
+    assert res.num_iterations <= res0.num_iterations, (res.num_iterations, res0.num_iterations)
+    assert float((hw - h.double()).abs().max()) < 1e-4  # the same head (h is stored in FP32)
+    s.close()
+    ws.close()
