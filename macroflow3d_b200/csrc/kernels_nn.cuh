@@ -83,14 +83,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 __device__ __forceinline__ void nn_mbar_init(uint64_t* bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sm_u32(bar)), "r"(count) : "memory");
 }
-// bounded wait on an mbarrier phase; false when it gave up
+// bounded wait on an mbarrier phase; false when it gave up.  Each try suspends the thread for
+// up to 2 us unless the phase completes first (fewer spinning instructions); at most 2^20 tries.
 __device__ __forceinline__ bool nn_mbar_wait(uint64_t* bar, unsigned parity) {
     const uint32_t a = sm_u32(bar);
-    for (int it = 0; it < (1 << 22); ++it) {
+    for (int it = 0; it < (1 << 20); ++it) {
         uint32_t ok;
-        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
                      : "=r"(ok)
-                     : "r"(a), "r"(parity)
+                     : "r"(a), "r"(parity), "r"(2000u)
                      : "memory");
         if (ok) return true;
     }
@@ -129,7 +130,7 @@ __host__ __device__ constexpr size_t conv_smem(int cin, int cout) {
     return 2 * ((size_t)CONV_TM * cin * 2 + (size_t)cout * cin * 2) + 64;
 }
 __host__ __device__ constexpr uint32_t tmem_cols(int cout) {
-    return cout <= 32 ? 32u : cout <= 64 ? 64u : cout <= 128 ? 128u : 256u;
+    return cout <= 32 ? 32u : cout <= 64 ? 64u : cout <= 128 ? 128u : cout <= 256 ? 256u : 512u;
 }
 
 __global__ void __launch_bounds__(CONV_NT) conv3d_tc_kernel(const ConvArgs a) {
@@ -285,57 +286,398 @@ __global__ void __launch_bounds__(CONV_NT) conv3d_tc_kernel(const ConvArgs a) {
     }
 }
 
+// ---- conv3d_brick_kernel: the same convolution with the halo staged once per plane ----
+// A CTA owns a 16 x 16 voxel brick (two 8 x 16 UMMA M-tiles) and marches it through a z
+// range.  Producer warps stage each input plane of the brick plus a one-voxel halo
+// (18 x 18 voxels x cin) into a ring of 4 plane slots with cp.async (zero fill outside the
+// grid), one region per 8-channel half so that every tap's A operand is the same K-major
+// canonical layout at a shifted start address: rows of 8 voxels along x at 16 bytes, 8-row
+// groups (y) 18 x 16 = 288 bytes apart, the two channel halves of a 16-channel K-step one
+// region (18 x 18 x 16 = 5184 bytes) apart.  The weights of all 27 taps stay in shared memory.
+// One thread issues the 27 x cin/16 x 2 MMAs of an output plane into one of two TMEM
+// accumulator buffers and commits them; four epilogue warps drain the other buffer
+// meanwhile (bias, ReLU or mask, BF16 / FP32 store).  Every wait is bounded.
+constexpr int BR_MAXNP = 8;                    // input plane slots, at most
+constexpr int BR_PROD = 4, BR_EPI = 4;         // producer and epilogue warps
+constexpr int BR_NT = (BR_PROD + 1 + BR_EPI) * 32;
+// Brick geometry: A UMMA M-tiles of 8 x 16 voxels side by side in x (brick 8A x 16), a ring of
+// NP input plane slots, each (8A + 2) x 18 voxels x cin channels, one region per 8 channels.
+__host__ __device__ constexpr int brick_region(int A) { return (8 * A + 2) * 18 * 16; }
+__host__ __device__ constexpr size_t brick_slot_bytes(int A, int cin) { return (size_t)brick_region(A) * (cin / 8); }
+__host__ __device__ constexpr size_t brick_smem(int A, int NP, int cin, int coutp) {
+    return (size_t)27 * coutp * cin * 2 + NP * brick_slot_bytes(A, cin) + 256;
+}
+__host__ __device__ constexpr uint32_t brick_tmem_cols(int A, int coutp) { return tmem_cols(2 * A * coutp); }
+
+// K-major descriptor with explicit leading / stride byte offsets
+__device__ __forceinline__ uint64_t kdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void nn_mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(sm_u32(bar)) : "memory");
+}
+
+struct BrickArgs {
+    int A, NP;        // M-tiles per brick row, input plane slots
+    int co0, coutp;   // the output channels [co0, co0 + coutp) of a.cout computed by this launch
+    int zchunk;       // planes per brick
+};
+
+template <int A>
+__global__ void __launch_bounds__(BR_NT, 1) conv3d_brick_kernel(const ConvArgs a, const BrickArgs g) {
+    extern __shared__ __align__(1024) unsigned char br_sm[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int cin = a.cin, ctot = a.cout, nhg = cin / 8;
+    const int NP = g.NP, co0 = g.co0, coutp = g.coutp, zchunk = g.zchunk;
+    const int W = 8 * A + 2;                       // slot width in voxels
+    const int REG = brick_region(A);               // bytes of one 8-channel region
+    const size_t SLOT = brick_slot_bytes(A, cin);
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    unsigned char* wsm = br_sm;                                   // weights: [t][hg][coutp] x 16 B
+    unsigned char* slots = br_sm + (size_t)27 * coutp * cin * 2;  // NP plane slots
+    uint64_t* bars = reinterpret_cast<uint64_t*>(slots + NP * SLOT);
+    uint64_t* full = bars;                 // [NP] plane staged (BR_PROD*32 arrivals)
+    uint64_t* empty = bars + BR_MAXNP;     // [NP] plane no longer read (MMA commit)
+    uint64_t* tfull = bars + 2 * BR_MAXNP; // [2] accumulator ready (MMA commit)
+    uint64_t* tempty = tfull + 2;          // [2] accumulator drained (BR_EPI*32 arrivals)
+    uint64_t* drain = tempty + 2;          // [1] every MMA of the CTA done (teardown)
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+    int* s_fail = reinterpret_cast<int*>(tmem_slot + 1);
+    const uint32_t ncols = brick_tmem_cols(A, coutp);
+    const int mma_warp = BR_PROD;
+
+    // weights of every tap (output channels co0..) in the canonical B layout: rows co at
+    // 16 B, 8-row groups 128 B apart, one region of coutp rows per 8 input channels
+    for (int q = tid; q < 27 * coutp * nhg; q += BR_NT) {
+        const int t = q / (coutp * nhg), r = q % (coutp * nhg), n = r / nhg, hg = r % nhg;
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(a.w + ((size_t)(co0 + n) * 27 + t) * cin) + hg);
+        *reinterpret_cast<uint4*>(wsm + ((size_t)(t * nhg + hg) * coutp + n) * 16) = v;
+    }
+    if (warp == mma_warp) {
+        tmem_alloc(tmem_slot, ncols);
+        tmem_relinquish();
+    }
+    if (tid == 0) {
+        for (int i = 0; i < NP; ++i) {
+            nn_mbar_init(&full[i], BR_PROD * 32);
+            nn_mbar_init(&empty[i], 1);
+        }
+        for (int i = 0; i < 2; ++i) {
+            nn_mbar_init(&tfull[i], 1);
+            nn_mbar_init(&tempty[i], BR_EPI * 32);
+        }
+        nn_mbar_init(drain, 1);
+        *s_fail = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); // weights -> tensor core
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    const int bw = 8 * A;
+    const int bx = (nx + bw - 1) / bw, by = (ny + 15) / 16, nzc = (nz + zchunk - 1) / zchunk;
+    const int nbricks = bx * by * nzc;
+    bool fail = false;
+
+    if (warp < BR_PROD) {
+        // ---------------- producers: the brick's input planes, in order ----------------
+        // The copies of plane p are committed as one group; the previous plane's group is then
+        // waited for, fenced towards the tensor core's proxy and announced, so that one plane's
+        // copies are always in flight while the previous one is published.
+        unsigned pc = 0;          // planes staged so far (ring position)
+        const int K = NP - 3;     // planes whose copies stay in flight (3 slots are being read)
+        int pend[BR_MAXNP], np_ = 0, ph = 0; // committed, not yet announced slots (oldest at ph)
+        const int nchunk = nhg * W * 18;
+        // wait until at most n copy groups of this thread are pending
+        auto wait_groups = [](int n) {
+            switch (n) {
+            case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
+            case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
+            case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
+            case 3: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
+            case 4: asm volatile("cp.async.wait_group 4;" ::: "memory"); break;
+            default: asm volatile("cp.async.wait_group 5;" ::: "memory"); break;
+            }
+        };
+        // announce the oldest pending plane once its copies have landed
+        auto publish_oldest = [&]() {
+            wait_groups(np_ - 1);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); // generic -> async proxy
+            nn_mbar_arrive(&full[pend[ph]]);
+            ph = (ph + 1) % BR_MAXNP;
+            --np_;
+        };
+        for (int br = blockIdx.x; br < nbricks && !fail; br += gridDim.x) {
+            const int col = br % (bx * by), zc = br / (bx * by);
+            const int x0 = (col % bx) * bw, y0 = (col / bx) * 16;
+            const int z0 = zc * zchunk, z1 = min(nz, z0 + zchunk);
+            for (int p = z0 - 1; p <= z1 && !fail; ++p, ++pc) {
+                const int sl = (int)(pc % NP);
+                if (pc >= (unsigned)NP) { // one lane per warp waits for the slot, the warp follows
+                    bool ok = lane == 0 ? nn_mbar_wait(&empty[sl], ((pc / NP) - 1) & 1u) : true;
+                    ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+                    if (!ok) {
+                        fail = true;
+                        break;
+                    }
+                }
+                const uint32_t base = sm_u32(slots + (size_t)sl * SLOT);
+                const bool pin = p >= 0 && p < nz;
+                for (int q = tid; q < nchunk; q += BR_PROD * 32) {
+                    const int hg = q / (W * 18), r = q % (W * 18), yy = r / W, xx = r % W;
+                    const int gx = x0 - 1 + xx, gy = y0 - 1 + yy;
+                    const bool ok = pin && gx >= 0 && gx < nx && gy >= 0 && gy < ny;
+                    const __nv_bfloat16* src = ok ? a.x + (((size_t)p * ny + gy) * nx + gx) * cin + hg * 8 : a.x;
+                    cp_async16(base + (uint32_t)(hg * REG + r * 16), src, ok);
+                }
+                asm volatile("cp.async.commit_group;" ::: "memory");
+                pend[(ph + np_) % BR_MAXNP] = sl;
+                ++np_;
+                while (np_ > K) publish_oldest();
+            }
+        }
+        while (np_ > 0) publish_oldest(); // the last planes
+        if (fail) atomicExch(s_fail, 1);
+    } else if (warp == mma_warp) {
+        // ---------------- MMA issuer (one thread) ----------------
+        if (lane == 0) {
+            const uint32_t idesc = idesc_bf16(CONV_TM, coutp);
+            const uint64_t bbase = kdesc(sm_u32(wsm), (uint32_t)(coutp * 16), 128u);
+            unsigned pc = 0, pw = 0; // planes waited for, output planes done
+            for (int br = blockIdx.x; br < nbricks && !fail; br += gridDim.x) {
+                const int zc = br / (bx * by);
+                const int z0 = zc * zchunk, z1 = min(nz, z0 + zchunk);
+                const unsigned pfirst = pc; // ring position of plane z0 - 1
+                for (int k = 0; k < 2 && !fail; ++k, ++pc)
+                    if (!nn_mbar_wait(&full[pc % NP], (pc / NP) & 1u)) fail = true;
+                for (int z = z0; z < z1 && !fail; ++z, ++pw) {
+                    if (!nn_mbar_wait(&full[pc % NP], (pc / NP) & 1u)) { // plane z + 1
+                        fail = true;
+                        break;
+                    }
+                    ++pc;
+                    const int tb = (int)(pw & 1u);
+                    if (pw >= 2 && !nn_mbar_wait(&tempty[tb], ((pw / 2) - 1) & 1u)) {
+                        fail = true;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t dacc = tmem + (uint32_t)(tb * A * coutp);
+                    // descriptors differ only in their start address (bits 0-13, in 16-byte
+                    // units): one base per operand, offsets added
+                    for (int dz = -1; dz <= 1; ++dz) {
+                        const unsigned pr = pfirst + (unsigned)(z - z0 + 1 + dz); // ring position of plane z + dz
+                        const uint64_t abase = kdesc(sm_u32(slots + (size_t)(pr % NP) * SLOT), (uint32_t)REG,
+                                                     (uint32_t)(W * 16));
+                        const int tz = (dz + 1) * 9;
+                        for (int s2 = 0; s2 < cin / 16; ++s2) {
+                            const uint64_t a_s = abase + (uint64_t)(2 * s2 * (REG >> 4));
+                            const uint64_t b_s = bbase + (uint64_t)(2 * s2 * coutp);
+#pragma unroll
+                            for (int tyx = 0; tyx < 9; ++tyx) {
+                                const int dy = tyx / 3, dx = tyx % 3; // 0..2: offsets + 1
+                                const uint64_t bd = b_s + (uint64_t)((tz + tyx) * nhg * coutp);
+                                // every tile's first product of the plane overwrites its accumulator
+                                const uint32_t acc = (dz > -1 || s2 > 0 || tyx > 0) ? 1u : 0u;
+#pragma unroll
+                                for (int j = 0; j < A; ++j)
+                                    umma_bf16(dacc + (uint32_t)(j * coutp), a_s + (uint64_t)(dy * W + dx + 8 * j), bd,
+                                              idesc, acc);
+                            }
+                        }
+                    }
+                    umma_commit(&tfull[tb]);
+                    // plane z - 1 is read by no later output plane of this brick
+                    umma_commit(&empty[(pfirst + (unsigned)(z - z0)) % NP]);
+                }
+                if (!fail) { // the brick's last two planes (z1 - 1, z1) are released too
+                    umma_commit(&empty[(pfirst + (unsigned)(z1 - z0)) % NP]);
+                    umma_commit(&empty[(pfirst + (unsigned)(z1 - z0 + 1)) % NP]);
+                }
+            }
+            if (fail) atomicExch(s_fail, 1);
+        }
+    } else {
+        // ---------------- epilogue warps: TMEM -> registers -> global ----------------
+        const int q = warp & 3;      // TMEM lane quarter this warp may access
+        const int m = q * 32 + lane; // row of an M-tile: x = m % 8, y = m / 8
+        unsigned pw = 0;
+        for (int br = blockIdx.x; br < nbricks && !fail; br += gridDim.x) {
+            const int col = br % (bx * by), zc = br / (bx * by);
+            const int x0 = (col % bx) * bw, y0 = (col / bx) * 16;
+            const int z0 = zc * zchunk, z1 = min(nz, z0 + zchunk);
+            for (int z = z0; z < z1 && !fail; ++z, ++pw) {
+                const int tb = (int)(pw & 1u);
+                // one lane waits, the warp follows (the TMEM loads below are warp-collective)
+                bool ok = lane == 0 ? nn_mbar_wait(&tfull[tb], (pw / 2) & 1u) : true;
+                ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+                if (!ok) {
+                    fail = true;
+                    break;
+                }
+                tc_fence_after();
+                for (int j = 0; j < A; ++j) {
+                    const int gx = x0 + 8 * j + (m & 7), gy = y0 + (m >> 3);
+                    const bool vin = gx < nx && gy < ny;
+                    const size_t v = ((size_t)z * ny + gy) * nx + gx;
+                    for (int c0 = 0; c0 < coutp; c0 += 16) {
+                        float acc[16];
+                        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(tb * A * coutp + j * coutp + c0), acc);
+                        if (!vin) continue;
+                        const int cg = co0 + c0; // channel in the full output
+                        if (a.bias)
+#pragma unroll
+                            for (int i = 0; i < 16; ++i) acc[i] += __ldg(a.bias + cg + i);
+                        if (a.relu)
+#pragma unroll
+                            for (int i = 0; i < 16; ++i) acc[i] = fmaxf(acc[i], 0.f);
+                        if (a.mask) {
+                            const uint4* mp = reinterpret_cast<const uint4*>(a.mask + v * ctot + cg);
+                            const uint4 m0 = __ldg(mp), m1 = __ldg(mp + 1);
+                            const __nv_bfloat16* mb0 = reinterpret_cast<const __nv_bfloat16*>(&m0);
+                            const __nv_bfloat16* mb1 = reinterpret_cast<const __nv_bfloat16*>(&m1);
+#pragma unroll
+                            for (int i = 0; i < 8; ++i) {
+                                if (!(__bfloat162float(mb0[i]) > 0.f)) acc[i] = 0.f;
+                                if (!(__bfloat162float(mb1[i]) > 0.f)) acc[8 + i] = 0.f;
+                            }
+                        }
+                        if (a.y_f32) {
+                            float4* yp = reinterpret_cast<float4*>(static_cast<float*>(a.y) + v * ctot + cg);
+#pragma unroll
+                            for (int i = 0; i < 4; ++i)
+                                yp[i] = make_float4(acc[4 * i], acc[4 * i + 1], acc[4 * i + 2], acc[4 * i + 3]);
+                        } else {
+                            __align__(16) __nv_bfloat16 o[16];
+#pragma unroll
+                            for (int i = 0; i < 16; ++i) o[i] = __float2bfloat16(acc[i]);
+                            uint4* yp = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(a.y) + v * ctot + cg);
+                            yp[0] = reinterpret_cast<const uint4*>(o)[0];
+                            yp[1] = reinterpret_cast<const uint4*>(o)[1];
+                        }
+                    }
+                }
+                tc_fence_before();
+                nn_mbar_arrive(&tempty[tb]);
+            }
+        }
+        if (fail) atomicExch(s_fail, 1);
+    }
+    // ---- teardown: every role has stopped issuing; the MMAs still in flight are waited for
+    // (one more commit tracks all of them) before the accumulator is released ----
+    __syncthreads();
+    if (warp == mma_warp && lane == 0) {
+        umma_commit(drain);
+        if (!nn_mbar_wait(drain, 0u)) atomicExch(s_fail, 1);
+    }
+    __syncthreads();
+    if (*s_fail && tid == 0) atomicExch(a.err, 1);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == mma_warp) {
+        tc_fence_after();
+        tmem_dealloc(tmem, ncols);
+    }
+}
+
 // ---- weight gradient (CUDA cores, FP32): dW[co][t][ci] = sum_v dY[v][co] X[v + off(t)][ci] ----
 // One CTA per (tap, voxel chunk); the CTA's partial goes to part[chunk][co][t][ci] and
-// wgrad_reduce_kernel adds the chunks in order (deterministic).
+// wgrad_reduce_kernel adds the chunks in order (deterministic).  Each thread owns 4 x 4
+// (co, ci) outputs; when the layer has fewer than 256 such tiles, G thread groups split the
+// staged voxels and their sums are added in shared memory at the end.
 constexpr int WG_NT = 256;
 constexpr int WG_VOX = 32; // voxels staged per step
 __global__ void __launch_bounds__(WG_NT) wgrad_kernel(const __nv_bfloat16* __restrict__ x,
                                                       const __nv_bfloat16* __restrict__ dy, float* __restrict__ part,
                                                       int nx, int ny, int nz, int cin, int cout, int vox_per_chunk) {
-    __shared__ float sx[WG_VOX][CONV_MAXC];
-    __shared__ float sd[WG_VOX][CONV_MAXC];
+    __shared__ __align__(16) float sx[WG_VOX][CONV_MAXC];
+    __shared__ __align__(16) float sd[WG_VOX][CONV_MAXC];
+    __shared__ __align__(16) float red[WG_NT * 16];
     const int t = blockIdx.x, chunk = blockIdx.y;
     const int dz = t / 9 - 1, dyo = (t / 3) % 3 - 1, dxo = t % 3 - 1;
     const long long V = (long long)nx * ny * nz;
     const long long v0 = (long long)chunk * vox_per_chunk, v1 = min(V, v0 + vox_per_chunk);
-    // thread -> (co, ci) pairs: cout * cin outputs, WG_NT threads
-    const int npair = cout * cin;
-    float acc[32]; // cout * cin <= 32 * WG_NT
+    const int tci = cin / 4, ntile = (cout / 4) * tci;
+    const int G = ntile >= WG_NT ? 1 : WG_NT / ntile; // thread groups over the voxels
+    const int per = (ntile + WG_NT - 1) / WG_NT;      // tiles per thread (G == 1)
+    const int tid = threadIdx.x, grp = tid / (WG_NT / G), tin = tid % (WG_NT / G);
+    const bool active = tid < G * (WG_NT / G) && (G > 1 ? tin < ntile : true);
+    float acc[2][16];
 #pragma unroll
-    for (int i = 0; i < 32; ++i) acc[i] = 0.f;
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int i = 0; i < 16; ++i) acc[u][i] = 0.f;
     for (long long vb = v0; vb < v1; vb += WG_VOX) {
         __syncthreads();
-        for (int e = threadIdx.x; e < WG_VOX * cin; e += WG_NT) {
-            const int q = e / cin, c = e % cin;
+        for (int e = tid; e < WG_VOX * (cin / 8); e += WG_NT) {
+            const int q = e / (cin / 8), c8 = e % (cin / 8);
             const long long v = vb + q;
-            float val = 0.f;
+            uint4 raw = make_uint4(0u, 0u, 0u, 0u);
             if (v < v1) {
                 const int i = (int)(v % nx) + dxo, j = (int)((v / nx) % ny) + dyo, k = (int)(v / ((long long)nx * ny)) + dz;
                 if (i >= 0 && i < nx && j >= 0 && j < ny && k >= 0 && k < nz)
-                    val = __bfloat162float(x[((size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k)) * cin + c]);
+                    raw = __ldg(reinterpret_cast<const uint4*>(x + ((size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k)) * cin) + c8);
             }
-            sx[q][c] = val;
+            const __nv_bfloat16* b = reinterpret_cast<const __nv_bfloat16*>(&raw);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) sx[q][c8 * 8 + u] = __bfloat162float(b[u]);
         }
-        for (int e = threadIdx.x; e < WG_VOX * cout; e += WG_NT) {
-            const int q = e / cout, c = e % cout;
+        for (int e = tid; e < WG_VOX * (cout / 8); e += WG_NT) {
+            const int q = e / (cout / 8), c8 = e % (cout / 8);
             const long long v = vb + q;
-            sd[q][c] = v < v1 ? __bfloat162float(dy[(size_t)v * cout + c]) : 0.f;
+            uint4 raw = make_uint4(0u, 0u, 0u, 0u);
+            if (v < v1) raw = __ldg(reinterpret_cast<const uint4*>(dy + (size_t)v * cout) + c8);
+            const __nv_bfloat16* b = reinterpret_cast<const __nv_bfloat16*>(&raw);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) sd[q][c8 * 8 + u] = __bfloat162float(b[u]);
         }
         __syncthreads();
-        int k = 0;
-        for (int p = threadIdx.x; p < npair; p += WG_NT, ++k) {
-            const int co = p / cin, ci = p % cin;
-            float s = 0.f;
-#pragma unroll 8
-            for (int q = 0; q < WG_VOX; ++q) s += sd[q][co] * sx[q][ci];
-            acc[k] += s;
+        if (!active) continue;
+        for (int u = 0; u < per && u < 2; ++u) {
+            const int tile = G > 1 ? tin : tid + u * WG_NT;
+            if (tile >= ntile) break;
+            const int co0 = (tile / tci) * 4, ci0 = (tile % tci) * 4;
+            for (int q = grp; q < WG_VOX; q += G) {
+                const float4 d4 = *reinterpret_cast<const float4*>(&sd[q][co0]);
+                const float4 x4 = *reinterpret_cast<const float4*>(&sx[q][ci0]);
+                const float dv[4] = {d4.x, d4.y, d4.z, d4.w}, xv[4] = {x4.x, x4.y, x4.z, x4.w};
+#pragma unroll
+                for (int a2 = 0; a2 < 4; ++a2)
+#pragma unroll
+                    for (int b2 = 0; b2 < 4; ++b2) acc[u][a2 * 4 + b2] += dv[a2] * xv[b2];
+            }
         }
     }
-    int k = 0;
-    for (int p = threadIdx.x; p < npair; p += WG_NT, ++k) {
-        const int co = p / cin, ci = p % cin;
-        part[((size_t)chunk * cout + co) * 27 * cin + (size_t)t * cin + ci] = acc[k];
+    // sum the G groups (index order), then store the tile
+    if (G > 1) {
+        __syncthreads();
+        if (active)
+#pragma unroll
+            for (int i = 0; i < 16; ++i) red[tid * 16 + i] = acc[0][i];
+        __syncthreads();
+        if (active && grp == 0) {
+            for (int g2 = 1; g2 < G; ++g2)
+#pragma unroll
+                for (int i = 0; i < 16; ++i) acc[0][i] += red[(g2 * (WG_NT / G) + tin) * 16 + i];
+        }
+    }
+    if (!active || (G > 1 && grp != 0)) return;
+    for (int u = 0; u < per && u < 2; ++u) {
+        const int tile = G > 1 ? tin : tid + u * WG_NT;
+        if (tile >= ntile) break;
+        const int co0 = (tile / tci) * 4, ci0 = (tile % tci) * 4;
+#pragma unroll
+        for (int a2 = 0; a2 < 4; ++a2)
+#pragma unroll
+            for (int b2 = 0; b2 < 4; ++b2)
+                part[((size_t)chunk * cout + co0 + a2) * 27 * cin + (size_t)t * cin + ci0 + b2] = acc[u][a2 * 4 + b2];
     }
 }
 
@@ -411,21 +753,26 @@ __global__ void pool_bwd_kernel(const __nv_bfloat16* __restrict__ dy, float* __r
         dx_acc[e] += 0.125f * __bfloat162float(dy[P * C + c]);
     }
 }
-// cat[v] = (coarse[parent(v)] (Ca channels), skip[v] (Cb channels)); fine grid (nx, ny, nz)
+// cat[v] = (coarse[parent(v)] (Ca channels), skip[v] (Cb channels)); fine grid (nx, ny, nz);
+// one thread per 8-channel chunk (Ca, Cb multiples of 8)
 __global__ void upcat_kernel(const __nv_bfloat16* __restrict__ coarse, const __nv_bfloat16* __restrict__ skip,
                              __nv_bfloat16* __restrict__ cat, int nx, int ny, int nz, int Ca, int Cb) {
-    const int C = Ca + Cb, cx = nx / 2, cy = ny / 2;
-    const size_t n = (size_t)nx * ny * nz * C;
+    const int qa = Ca / 8, qb = Cb / 8, Q = qa + qb, cx = nx / 2, cy = ny / 2;
+    const size_t n = (size_t)nx * ny * nz * Q;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-        const int c = (int)(e % C);
-        const size_t v = e / C;
-        if (c < Ca) {
-            const int i = (int)(v % nx), j = (int)((v / nx) % ny), k = (int)(v / ((size_t)nx * ny));
+        const int q = (int)(e % Q);
+        const size_t v = e / Q;
+        uint4 val;
+        if (q < qa) {
+            const int i = (int)(v % nx);
+            const size_t r = v / nx;
+            const int j = (int)(r % ny), k = (int)(r / ny);
             const size_t P = (size_t)(i >> 1) + (size_t)cx * ((size_t)(j >> 1) + (size_t)cy * (k >> 1));
-            cat[e] = coarse[P * Ca + c];
+            val = __ldg(reinterpret_cast<const uint4*>(coarse + P * Ca) + q);
         } else {
-            cat[e] = skip[v * Cb + (c - Ca)];
+            val = __ldg(reinterpret_cast<const uint4*>(skip + v * Cb) + (q - qa));
         }
+        reinterpret_cast<uint4*>(cat + v * (Ca + Cb))[q] = val;
     }
 }
 // gradient of upcat: dcoarse[P] = sum over the 8 children of dcat[child][0:Ca];

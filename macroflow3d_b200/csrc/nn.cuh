@@ -21,6 +21,7 @@ namespace mf3d {
 namespace nn {
 
 constexpr double kTargetScale = 0.1; // out[:, 0] = (h - h_lin) / kTargetScale
+constexpr size_t kBrickSmemMax = 220 * 1024; // shared memory of the brick convolution, at most
 
 struct LayerSpec {
     int cin, cout, level, relu;
@@ -188,9 +189,47 @@ class WarmStartNet {
         a.relu = relu;
         a.y_f32 = y_f32;
         a.err = err;
+        // brick kernel (halo staged once per plane) when a geometry fits: the output channels
+        // in as few launches as possible (1, 2 or 4), then two or one M-tiles per brick, then
+        // four or three plane slots
+        // More M-tiles per brick (A) give the tensor core more independent accumulators to
+        // interleave; no wider than the grid.
+        int amax = 1;
+        while (amax < 8 && 8 * amax * 2 <= std::max(8, d.nx)) amax *= 2;
+        for (int split = 1; split <= 4; split *= 2)
+            for (int A = amax; A >= 1; A /= 2)
+                for (int NP = 8; NP >= 3; --NP) { // 3 slots read, NP - 3 loading ahead
+                    const int coutp = cout / split;
+                    if (cout % split || coutp % 16 || cin > 128) continue;
+                    if (brick_smem(A, NP, cin, coutp) > kBrickSmemMax || 2 * A * coutp > 512) continue;
+                    if (A > 1 && NP < 5 && brick_smem(A / 2, 5, cin, coutp) <= kBrickSmemMax) continue; // keep lookahead
+                    auto kern = A == 8 ? conv3d_brick_kernel<8>
+                              : A == 4 ? conv3d_brick_kernel<4>
+                              : A == 2 ? conv3d_brick_kernel<2> : conv3d_brick_kernel<1>;
+                    MF3D_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBrickSmemMax));
+                    const int cols = ((d.nx + 8 * A - 1) / (8 * A)) * ((d.ny + 15) / 16);
+                    const int nzc = std::max(1, std::min(std::max(1, d.nz / 4), (2 * num_sms() + cols - 1) / cols));
+                    BrickArgs g{};
+                    g.A = A;
+                    g.NP = NP;
+                    g.coutp = coutp;
+                    g.zchunk = (d.nz + nzc - 1) / nzc;
+                    const long long bricks = (long long)cols * ((d.nz + g.zchunk - 1) / g.zchunk);
+                    const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(bricks, num_sms()));
+                    for (int c = 0; c < split; ++c) {
+                        g.co0 = c * coutp;
+                        kern<<<grid, BR_NT, brick_smem(A, NP, cin, coutp), s>>>(a, g);
+                        MF3D_LAUNCH_CK();
+                    }
+                    return;
+                }
         const size_t smem = conv_smem(cin, cout);
         MF3D_CK(cudaFuncSetAttribute(conv3d_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)conv_smem(CONV_MAXC, CONV_MAXC)));
+        // all of the unified L1 as shared memory: without it the driver sizes the carveout for
+        // the largest allowed allocation and keeps one CTA per SM
+        MF3D_CK(cudaFuncSetAttribute(conv3d_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared));
         int occ = 0;
         MF3D_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, conv3d_tc_kernel, CONV_NT, smem));
         // no more CTAs per SM than their TMEM accumulators fit in (512 columns)
@@ -211,7 +250,7 @@ class WarmStartNet {
         int nch = (int)((V + vpc - 1) / vpc);
         const size_t wn = (size_t)cout * 27 * cin;
         if ((size_t)nch * wn > part_floats) throw Error(MF3D_E_INVALID, "weight-gradient scratch too small");
-        if (cout * cin > 32 * WG_NT) throw Error(MF3D_E_INVALID, "layer too wide for the weight gradient");
+        if (cout * cin > 2 * 16 * WG_NT) throw Error(MF3D_E_INVALID, "layer too wide for the weight gradient");
         wgrad_kernel<<<dim3(27, nch), WG_NT, 0, s>>>(x, dy, part, d.nx, d.ny, d.nz, cin, cout, vpc);
         MF3D_LAUNCH_CK();
         wgrad_reduce_kernel<<<ew_grid(wn), 256, 0, s>>>(part, nch, wn, dw, accumulate);
@@ -319,13 +358,13 @@ class WarmStartNet {
         MF3D_LAUNCH_CK();
         layer(s, 6, d3, b.p2, b.a6);
         layer(s, 7, d3, b.a6, b.e3);
-        upcat_kernel<<<ew_grid(d2.v() * 128), 256, 0, s>>>(b.e3, b.e2, b.c2, d2.nx, d2.ny, d2.nz, 64, 64);
+        upcat_kernel<<<ew_grid(d2.v() * 16), 256, 0, s>>>(b.e3, b.e2, b.c2, d2.nx, d2.ny, d2.nz, 64, 64);
         MF3D_LAUNCH_CK();
         layer(s, 8, d2, b.c2, b.d2);
-        upcat_kernel<<<ew_grid(d1.v() * 96), 256, 0, s>>>(b.d2, b.e1, b.c1, d1.nx, d1.ny, d1.nz, 64, 32);
+        upcat_kernel<<<ew_grid(d1.v() * 12), 256, 0, s>>>(b.d2, b.e1, b.c1, d1.nx, d1.ny, d1.nz, 64, 32);
         MF3D_LAUNCH_CK();
         layer(s, 9, d1, b.c1, b.d1);
-        upcat_kernel<<<ew_grid(d0.v() * 48), 256, 0, s>>>(b.d1, b.e0, b.c0, d0.nx, d0.ny, d0.nz, 32, 16);
+        upcat_kernel<<<ew_grid(d0.v() * 6), 256, 0, s>>>(b.d1, b.e0, b.c0, d0.nx, d0.ny, d0.nz, 32, 16);
         MF3D_LAUNCH_CK();
         layer(s, 10, d0, b.c0, b.d0);
         layer(s, 11, d0, b.d0, b.out, 1);
