@@ -117,14 +117,16 @@ def solver_cfg(M, n, precision, rtol=1e-10):
                              conv_norm=M.CONV_B, precision=precision, use_graph=USE_GRAPH)
 
 
-def run_steps(M, n, K, precision, steps, warmup, dist_ctx=None):
-    """Times `steps` device-resident steps; returns dict with per-step ms and last result."""
+def run_steps(M, n, K, precision, steps, warmup, dist_ctx=None, warmstart=None):
+    """Times `steps` device-resident steps; returns dict with per-step ms and last result.
+    With `warmstart`, every step also runs the network's inference and solves from its guess."""
     import torch
     g = M.Grid3D(n, n, n, 1.0)
     bc = M.BCSpec.darcy_x()
     stream = torch.cuda.current_stream()
     s = M.HeadSolver(g, bc, solver_cfg(M, n, precision), stream=stream.cuda_stream)
     h = torch.empty_like(K)
+    x0 = torch.empty_like(K) if warmstart is not None else None
     su, sv, sw = M.velocity_sizes(g)
     U = torch.empty(su, dtype=torch.float64, device=K.device)
     V = torch.empty(sv, dtype=torch.float64, device=K.device)
@@ -132,7 +134,9 @@ def run_steps(M, n, K, precision, steps, warmup, dist_ctx=None):
 
     def step():
         s.set_K(K)
-        r = s.solve(h)
+        if warmstart is not None:
+            warmstart.predict(g, bc, K, x0)
+        r = s.solve(h, x0)
         M.compute_velocity_from_head(U, V, W, h, K, g, bc)
         return r
 
@@ -192,6 +196,56 @@ def e2e_steps(M, n, K_host, precision, steps, warmup):
     nbytes = K_host.numel() * 8
     s.close()
     return steps / (ms / 1e3), nbytes, nbytes
+
+
+def warmstart_eval(M, precision, seed):
+    """Config C5: the shipped network (trained on 2000 solver-generated pairs at 128^3) as the
+    PCG initial guess at 128^3 and 256^3 on held-out fields, against the zero guess and the
+    reference's x-linear guess; PCG runs to ||r||/||b|| <= 1e-10 in every case."""
+    import numpy as np
+    import torch
+    ws = M.WarmStart.pretrained()
+    bc = M.BCSpec.darcy_x()
+    stream = torch.cuda.current_stream()
+    cases = []
+    for n in (128, 256):
+        g = M.Grid3D(n, n, n, 1.0)
+        s = M.HeadSolver(g, bc, solver_cfg(M, n, precision), stream=stream.cuda_stream)
+        for k, (s2, lam) in enumerate([(1.0, 6.0), (2.5, 8.0), (4.0, 10.0)]):
+            K = M.generate_K_field(g, s2, (lam, lam, lam), seed=seed + 9_000_000 + 100 * n + k, n_modes=1000)
+            s.set_K(K)
+            h = torch.empty_like(K)
+            x0 = torch.zeros_like(K)
+            s.solve(h)  # warm-up of this grid's graph
+            r_lin = s.solve(h)
+            href = h.clone()
+            r_zero = s.solve(h, x0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ws.predict(g, bc, K, x0)
+            e0.record(stream)
+            ws.predict(g, bc, K, x0)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t_inf = e0.elapsed_time(e1)
+            err_nn = float((x0 - href).norm() / href.norm())
+            hl = torch.from_numpy(np.broadcast_to(1.0 - (np.arange(n) + 0.5) / n, (n, n, n)).copy()).to(K.device)
+            err_lin = float((hl - href).norm() / href.norm())
+            r_nn = s.solve(h, x0)
+            cases.append({"n": n, "sigma2": s2, "lambda": lam,
+                          "iterations": {"zero": r_zero.num_iterations, "linear": r_lin.num_iterations,
+                                         "learned": r_nn.num_iterations},
+                          "solve_ms": {"zero": round(r_zero.device_ms, 3), "linear": round(r_lin.device_ms, 3),
+                                       "learned_incl_inference": round(r_nn.device_ms + t_inf, 3)},
+                          "inference_ms": round(t_inf, 3),
+                          "guess_rel_error": {"zero": 1.0, "linear": err_lin, "learned": err_nn},
+                          "true_rel_residual_learned": r_nn.true_rel_residual,
+                          "head_rel_diff_learned_vs_linear": float((h - href).abs().max() / href.abs().max())})
+        s.close()
+    ws.close()
+    return {"network": "3-D U-Net, 4 levels, 16/32/64/64 channels, 3x3x3, BF16 / FP32 accumulate (tcgen05)",
+            "training": "2000 solver-generated pairs at 128^3, lnK variance U(0.5, 4), correlation length U(4, 12); "
+                        "3 epochs of Adam, minibatch 4 (macroflow3d_b200.warmstart_train)",
+            "held_out": "seeds outside the training set", "cases": cases}
 
 
 ENSEMBLE_EDGES = (64, 96, 128, 160)
@@ -373,6 +427,7 @@ def main():
     ap.add_argument("--profile-kernels", action="store_true", help="print per-kernel timings")
     ap.add_argument("--seed", type=int, default=20240601)
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched Monte Carlo ensemble")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned warm start records")
     ap.add_argument("--ensemble-only", action="store_true",
                     help="run only the batched Monte Carlo ensemble and print its record")
     ap.add_argument("--ensemble-count", type=int, default=128)
@@ -484,6 +539,19 @@ def main():
                        "d2h_bytes_per_step": bo}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(K.cpu().numpy(), n, iters64)
+    if rank == 0 and world == 1 and not args.no_learned:
+        ws = M.WarmStart.pretrained()
+        ol = run_steps(M, n, K, prec, args.steps, args.warmup, None, warmstart=ws)
+        v_l = args.steps / (ol["ms_total"] / 1e3)
+        line["learned_mixed"] = {"solves_per_s": round(v_l, 4), "iterations": ol["iters"][-1],
+                                 "true_rel_residual": ol["res"].true_rel_residual,
+                                 "step": "set-up from K + network inference + PCG from its guess + face velocity",
+                                 "speedup_vs_fp64_plain": round(v_l / line["fp64_plain"]["solves_per_s"], 3)
+                                 if "fp64_plain" in line else None,
+                                 "speedup_vs_mixed": round(v_l / value, 3)}
+        ol["solver"].close()
+        ws.close()
+        line["warm_start_c5"] = warmstart_eval(M, prec, args.seed)
     if rank == 0 and world == 1 and not args.no_ensemble:
         del K
         torch.cuda.empty_cache()

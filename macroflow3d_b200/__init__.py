@@ -307,8 +307,21 @@ class WarmStart:
         np.save(path, self.get_params())
 
     def load(self, path: str) -> None:
+        """Parameters from a .npy file: FP32, or BF16 bit patterns stored as uint16."""
         import numpy as np
-        self.set_params(np.load(path))
+        p = np.load(path)
+        if p.dtype == np.uint16:
+            p = (p.astype(np.uint32) << 16).view(np.float32)
+        self.set_params(p)
+
+    @classmethod
+    def pretrained(cls):
+        """The network trained on 2000 solver-generated pairs at 128^3 (lnK variance 0.5-4,
+        correlation length 4-12 cells; macroflow3d_b200.warmstart_train), shipped as BF16."""
+        import os
+        ws = cls(seed=0)
+        ws.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "warmstart_c5_bf16.npy"))
+        return ws
 
     @staticmethod
     def _f32_ptrs(arrays, n, what):
