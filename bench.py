@@ -94,10 +94,16 @@ class Clocks:
 
 
 def make_K(M, n, sigma2, lam, seed, device):
+    """lam: one correlation length, or (lambda_x, lambda_y, lambda_z)."""
     import torch
     g = M.Grid3D(n, n, n, 1.0)
+    lams = tuple(lam) if isinstance(lam, (tuple, list)) else (lam, lam, lam)
     with torch.cuda.device(device):
-        return M.generate_K_field(g, sigma2, (lam, lam, lam), seed=seed, n_modes=1000)
+        return M.generate_K_field(g, sigma2, lams, seed=seed, n_modes=1000)
+
+
+# the workloads: C2 (256^3, the headline), C1 (64^3 parity case), C3 (512^3, anisotropic)
+CONFIGS = {"c2": (256, 4.0, 8.0), "c1": (64, 1.0, 4.0), "c3": (512, 1.0, (16.0, 16.0, 4.0))}
 
 
 def levels_for(n):
@@ -419,7 +425,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS),
+                    help="c2: 256^3 sigma2 4 lambda 8 (default); c1: 64^3 sigma2 1 lambda 4; "
+                         "c3: 512^3 sigma2 1 lambda (16, 16, 4)")
+    ap.add_argument("--size", type=int, default=None, help="grid edge (overrides the config's)")
     ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32", "bf16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-compare", action="store_true")
@@ -452,9 +461,13 @@ def main():
         dist_ctx = dist
     else:
         torch.cuda.set_device(0)
-    n = args.size
-    sigma2, lam = 4.0, 8.0
-    config = {"workload": f"darcy_ccmg_pcg_{n}^3_sigma2_{sigma2:g}_lambda_{lam:g}",
+    n, sigma2, lam = CONFIGS[args.config]
+    if args.size is not None:
+        n = args.size
+    if args.config != "c2":  # the ensemble (C4) and warm-start (C5) records go with the headline run
+        args.no_ensemble = args.no_learned = True
+    lam_s = "x".join(f"{v:g}" for v in lam) if isinstance(lam, tuple) else f"{lam:g}"
+    config = {"workload": f"darcy_ccmg_pcg_{n}^3_sigma2_{sigma2:g}_lambda_{lam_s}",
               "grid": [n, n, n], "cells": n ** 3, "lnK": "gaussian, exponential covariance, 1000 modes",
               "tolerance": "||b-Ah||/||b|| <= 1e-10", "bc": "h=1 at x=0, h=0 at x=L, no-flow elsewhere",
               "step": "set-up from K + PCG + face velocity", "l2": "inputs larger than L2 (no flush)",
@@ -499,7 +512,7 @@ def main():
         ms = float(t.item())
     value = world * args.steps / (ms / 1e3)
     res = out["res"]
-    line = {"metric": "darcy_solves_per_s_256cubed_relres_1e-10", "value": round(value, 4),
+    line = {"metric": f"darcy_solves_per_s_{n}cubed_relres_1e-10", "value": round(value, 4),
             "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 outer / f32 V-cycle" if prec == M.PREC_FP32 else args.precision,
@@ -570,7 +583,7 @@ def reference_arm(args, n, sigma2, lam, config):
     import torch
     from oracle import oracle as O
     import macroflow3d_b200 as M
-    base = {"impl": "reference", "metric": "darcy_solves_per_s_256cubed_relres_1e-10", "unit": "solves/s",
+    base = {"impl": "reference", "metric": f"darcy_solves_per_s_{n}cubed_relres_1e-10", "unit": "solves/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded randomization-method lnK field)", "config": config}
