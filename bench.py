@@ -117,6 +117,25 @@ def levels_for(n):
 USE_GRAPH = 1
 
 
+# ---- replicas (N > 1): one independent solve per rank, no collective on the data path ----
+def replica_seed(base, rank):
+    """Each rank solves its own realisation: seed + rank (EnsembleRunner's seed + r)."""
+    return base + rank
+
+
+def max_over_ranks(dist_ctx, ms, device):
+    """The job's time is the slowest rank's (the only collective: one scalar all-reduce)."""
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist_ctx.all_reduce(t, op=dist_ctx.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_value(world, steps, ms):
+    """Whole-job solves/s: every rank ran `steps` solves within the slowest rank's `ms`."""
+    return world * steps / (ms / 1e3)
+
+
 def solver_cfg(M, n, precision, rtol=1e-10):
     return M.HeadSolveConfig(mg_levels=levels_for(n), mg_pre_smooth=2, mg_post_smooth=2,
                              mg_coarse_iters=50, cg_max_iter=500, cg_check_every=1, cg_rtol=rtol,
@@ -499,7 +518,7 @@ def main():
             dist_ctx.barrier()
             dist_ctx.destroy_process_group()
         return
-    K = make_K(M, n, sigma2, lam, args.seed + rank, torch.cuda.current_device())
+    K = make_K(M, n, sigma2, lam, replica_seed(args.seed, rank), torch.cuda.current_device())
     torch.cuda.synchronize()
 
     with Clocks(torch.cuda.current_device()) as clk:
@@ -507,10 +526,8 @@ def main():
     clocks = clk.summary()
     ms = out["ms_total"]
     if dist_ctx is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist_ctx.all_reduce(t, op=dist_ctx.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * args.steps / (ms / 1e3)
+        ms = max_over_ranks(dist_ctx, ms, "cuda")
+    value = replicas_value(world, args.steps, ms)
     res = out["res"]
     line = {"metric": f"darcy_solves_per_s_{n}cubed_relres_1e-10", "value": round(value, 4),
             "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
