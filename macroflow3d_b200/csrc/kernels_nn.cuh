@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(BR_NT, 1) conv3d_brick_kernel(const ConvArgs a
         // copies are always in flight while the previous one is published.
         unsigned pc = 0;          // planes staged so far (ring position)
         const int K = NP - 3;     // planes whose copies stay in flight (3 slots are being read)
-        int pend[BR_MAXNP], np_ = 0, ph = 0; // committed, not yet announced slots (oldest at ph)
+        int pend[BR_MAXNP] = {}, np_ = 0, ph = 0; // committed, not yet announced slots (oldest at ph)
         const int nchunk = nhg * W * 18;
         // wait until at most n copy groups of this thread are pending
         auto wait_groups = [](int n) {

@@ -6,6 +6,8 @@
 // finishes the x/r update also evaluates the stopping test and sets the CUDA-graph `while`
 // condition, so a whole solve is one graph launch with no host round trip.
 #pragma once
+#include <cstddef>
+
 #include "mf3d_device.cuh"
 
 namespace mf3d {
@@ -183,12 +185,6 @@ __device__ __forceinline__ void pupdate_body(size_t n, const TZ* __restrict__ z,
         p[c] = 1.0 * (double)z[c] + beta * p[c];
 }
 
-template <class TZ>
-__global__ void __launch_bounds__(PK_NT) pupdate_kernel(size_t n, const TZ* __restrict__ z, double* __restrict__ p,
-                                                        PcgState* st) {
-    pupdate_body<TZ>(n, z, p, st, blockIdx.x, gridDim.x);
-}
-
 // Ap = A p and <p, Ap>.
 template <class TC>
 __device__ __forceinline__ void matvec_dot_body(const LevelOp<TC>& L, const double* __restrict__ p,
@@ -210,11 +206,204 @@ __device__ __forceinline__ void matvec_dot_body(const LevelOp<TC>& L, const doub
     if (grid_sums<PK_NT, 1>(v, partials, ticket, vb.count, out, vb.id)) st->pAp = out[0];
 }
 
-template <class TC>
-__global__ void __launch_bounds__(PK_NT) matvec_dot_kernel(const LevelOp<TC> L, const double* __restrict__ p,
-                                                           double* __restrict__ Ap, PcgState* st,
-                                                           double* partials, unsigned* ticket, int zchunk) {
-    matvec_dot_body<TC>(L, p, Ap, st, partials, ticket, zchunk, hw_vblk());
+// The search-direction update of pupdate_body fused with matvec_dot_body: p_new = z + beta
+// p_old is formed once per cell from z and p_old and written once, instead of written by one
+// kernel and re-read by the next.  p_old and p_new live in two buffers that swap by iteration
+// parity (pcg_pbuf_in / pcg_pbuf_out): no CTA overwrites a value that another still reads.
+//
+// 2.5-D blocking: a CTA of 32 x 8 threads owns a 32 x 8 column tile and marches a z chunk.
+// Every thread stages, by cp.async into a ring of PMV_NS shared-memory slots, the z and p_old
+// of its own cell (and of the ring cells beside the tile that it is assigned) and its cell's
+// +x/+y/+z faces (the threads on the -x/-y edges also the -x/-y faces), three planes ahead of
+// the plane it applies: those copies are in flight while the CTA computes.  From a landed
+// slot each thread forms p_new of the cells it staged into a double-buffered slab (tile plus
+// one-cell ring); the stencil reads its x/y neighbours from the slab, its -z/+z values and
+// its -z face from registers.  One barrier per plane.  Cells outside a non-periodic axis are
+// staged as zeros (the operator's ghost value, p_new = 0); periodic axes wrap.  Arithmetic
+// per cell is that of pupdate_body and apply_A_cell, bit for bit.
+__device__ __forceinline__ const double* pcg_pbuf_in(int iter, const double* p0, const double* p1) {
+    return (iter & 1) ? p1 : p0;
+}
+__device__ __forceinline__ double* pcg_pbuf_out(int iter, double* p0, double* p1) { return (iter & 1) ? p0 : p1; }
+
+#ifndef MF3D_PMATVEC_MINB
+#define MF3D_PMATVEC_MINB 3 // resident CTAs per SM the register budget is cut for (72 registers)
+#endif
+#ifndef MF3D_PMATVEC_PERSM
+#define MF3D_PMATVEC_PERSM 8 // CTAs launched per SM (z chunks sized to match)
+#endif
+constexpr int PMV_TX = 32, PMV_TY = 8, PMV_NS = 4;
+
+template <class TZ> struct PmvSlot {
+    TZ z[PMV_TY + 2][PMV_TX + 2];     // tile and ring, row 0 / column 0 at j0-1 / i0-1
+    double p[PMV_TY + 2][PMV_TX + 2]; // p_old, same layout
+    double cx[PMV_TY][PMV_TX + 1];    // +x faces at column tx+1; column 0: the -x faces at i0
+    double cy[PMV_TY + 1][PMV_TX];    // +y faces at row ty+1; row 0: the -y faces at j0
+    double cz[PMV_TY][PMV_TX];        // +z faces
+};
+template <class TZ> constexpr size_t pmv_smem_bytes() {
+    return PMV_NS * sizeof(PmvSlot<TZ>) + 2 * sizeof(double) * (PMV_TY + 2) * (PMV_TX + 2);
+}
+
+// cp.async of B bytes (4 or 8); zeros when !ok (nothing is read then)
+template <int B> __device__ __forceinline__ void pmv_cp(void* dst, const void* src, bool ok) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src), "n"(B), "r"(ok ? B : 0)
+                 : "memory");
+}
+
+template <class TZ>
+__global__ void __launch_bounds__(PMV_TX * PMV_TY, MF3D_PMATVEC_MINB)
+    pmatvec_dot_kernel(const LevelOp<double> L, const TZ* __restrict__ z, double* p0, double* p1,
+                       double* __restrict__ Ap, PcgState* st, double* partials, unsigned* ticket, int zchunk) {
+    constexpr int W = PMV_TX + 2; // slab / staged-plane row pitch
+    extern __shared__ __align__(16) unsigned char pmv_sm[];
+    PmvSlot<TZ>* slot = reinterpret_cast<PmvSlot<TZ>*>(pmv_sm);
+    double* slab = reinterpret_cast<double*>(pmv_sm + PMV_NS * sizeof(PmvSlot<TZ>)); // [2][PMV_TY + 2][W]
+    const PcgState s = *st;
+    if (s.stop) return;
+    const bool first = s.iter == 0;
+    const double beta = first ? 0.0 : (s.rho_new - (s.flexible ? s.gamma : 0.0)) / s.rho_old;
+    const VBlk vb = hw_vblk();
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    if (vb.id == 0 && tx == 0 && ty == 0) st->beta = beta;
+    const double* __restrict__ pin = pcg_pbuf_in(s.iter, p0, p1);
+    double* __restrict__ pout = pcg_pbuf_out(s.iter, p0, p1);
+    const int nx = L.nx, ny = L.ny, nz = L.nz;
+    const size_t nxy = (size_t)nx * ny;
+    const int i0 = vb.x * PMV_TX, j0 = vb.y * PMV_TY, i = i0 + tx, j = j0 + ty;
+    const int k0 = vb.z * zchunk, k1 = min(k0 + zchunk, nz);
+    const bool own = i < nx && j < ny;
+    // Staging roles, fixed for the whole march: the thread's own cell, and at most one more
+    // (warp-uniform kind): warp 0 the ring row below the tile, warp PMV_TY-1 the row above,
+    // warp 1 lanes 0-15 the ring columns left and right, warp 1 lanes 16-23 the -x faces of
+    // the tile's first column, warp 2 the -y faces of its first row.
+    auto xy_of = [&](int ii, int jj, long long& g) {
+        const int a = wrap_or_out(ii, nx, L.per_x), b = wrap_or_out(jj, ny, L.per_y);
+        g = (long long)a + (long long)nx * b;
+        return a >= 0 && b >= 0;
+    };
+    long long gO, gE = 0;
+    const bool okO = xy_of(i, j, gO);
+    const int fO = (ty + 1) * W + tx + 1;
+    int kindE = 0, fE = 0; // 1: a ring cell at slab index fE; 2: a face into slot offset fE
+    bool okE = false;
+    const double* cb = L.cx; // kind 2: face of plane kk at cb + cs * kk
+    size_t cs = 0;
+    if (ty == 0 || ty == PMV_TY - 1) {
+        kindE = 1;
+        const int jj = ty == 0 ? j0 - 1 : j0 + PMV_TY;
+        fE = (ty == 0 ? 0 : PMV_TY + 1) * W + tx + 1;
+        okE = xy_of(i, jj, gE);
+    } else if (ty == 1 && tx < 16) {
+        kindE = 1;
+        const int side = tx >> 3, row = tx & 7;
+        fE = (row + 1) * W + (side ? PMV_TX + 1 : 0);
+        okE = xy_of(side ? i0 + PMV_TX : i0 - 1, j0 + row, gE);
+    } else if (ty == 1 && tx < 16 + PMV_TY) {
+        kindE = 2;
+        const int row = tx - 16, jj = j0 + row;
+        okE = jj < ny;
+        fE = (int)offsetof(PmvSlot<TZ>, cx) + row * (PMV_TX + 1) * 8;
+        if (i0 > 0) cb = L.cx + (i0 - 1) + (size_t)nx * jj, cs = nxy;
+        else if (L.per_x) cb = L.cx + (nx - 1) + (size_t)nx * jj, cs = nxy;
+        else cb = L.bxm + jj, cs = (size_t)ny;
+    } else if (ty == 2) {
+        kindE = 2;
+        okE = i < nx;
+        fE = (int)offsetof(PmvSlot<TZ>, cy) + tx * 8;
+        if (j0 > 0) cb = L.cy + i + (size_t)nx * (j0 - 1), cs = nxy;
+        else if (L.per_y) cb = L.cy + i + (size_t)nx * (ny - 1), cs = nxy;
+        else cb = L.bym + i, cs = (size_t)nx;
+    }
+    if (!okE && kindE == 2) cb = L.cx, cs = 0;
+    const size_t cO = own ? (size_t)i + (size_t)nx * j : 0; // own cell in plane 0
+    auto pval = [&](TZ zr, double pr) -> double {
+        const double zv = (double)zr;
+        return first ? zv : 1.0 * zv + beta * pr;
+    };
+    // one commit group per plane: z and p_old of the staged cells, the faces of the own cell
+    auto issue = [&](int kk) {
+        if (kk <= k1) {
+            PmvSlot<TZ>& S = slot[(unsigned)(kk - k0) % PMV_NS];
+            const int kz = wrap_or_out(kk, nz, L.per_z);
+            const long long zo = (long long)nxy * (kz < 0 ? 0 : kz);
+            const bool okO_k = okO && kz >= 0;
+            const size_t g = okO_k ? (size_t)(gO + zo) : 0;
+            pmv_cp<(int)sizeof(TZ)>(&S.z[0][0] + fO, z + g, okO_k);
+            pmv_cp<8>(&S.p[0][0] + fO, pin + g, okO_k && !first);
+            if (kindE == 1) {
+                const bool ok = okE && kz >= 0;
+                const size_t ge = ok ? (size_t)(gE + zo) : 0;
+                pmv_cp<(int)sizeof(TZ)>(&S.z[0][0] + fE, z + ge, ok);
+                pmv_cp<8>(&S.p[0][0] + fE, pin + ge, ok && !first);
+            }
+            if (kk < k1) {
+                if (own) {
+                    const size_t c = cO + nxy * kk;
+                    pmv_cp<8>(&S.cx[ty][tx + 1], L.cx + c, true);
+                    pmv_cp<8>(&S.cy[ty + 1][tx], L.cy + c, true);
+                    pmv_cp<8>(&S.cz[ty][tx], L.cz + c, true);
+                }
+                if (kindE == 2) pmv_cp<8>(reinterpret_cast<unsigned char*>(&S) + fE, cb + cs * kk, okE);
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    // p_new of the staged cells of the plane in S, into the slab D; returns the own cell's
+    auto form = [&](const PmvSlot<TZ>& S, double* D) -> double {
+        const double v = pval((&S.z[0][0])[fO], (&S.p[0][0])[fO]);
+        D[fO] = v;
+        if (kindE == 1) D[fE] = pval((&S.z[0][0])[fE], (&S.p[0][0])[fE]);
+        return v;
+    };
+    constexpr int SLAB = (PMV_TY + 2) * W;
+    double acc = 0.0, pb = 0.0, czm = 0.0;
+    size_t c = cO + nxy * k0;
+    if (own) { // the -z neighbour and the -z face of the first plane, read directly
+        const int kb = wrap_or_out(k0 - 1, nz, L.per_z);
+        if (kb >= 0) {
+            const size_t g = cO + nxy * kb;
+            pb = pval(__ldg(z + g), first ? 0.0 : __ldg(pin + g));
+        }
+        czm = k0 > 0 ? __ldg(L.cz + c - nxy)
+                     : (L.per_z ? __ldg(L.cz + c + (size_t)(nz - 1) * nxy) : __ldg(L.bzm + cO));
+    }
+    issue(k0);
+    issue(k0 + 1);
+    issue(k0 + 2);
+    asm volatile("cp.async.wait_group 2;" ::: "memory");
+    double pc = form(slot[0], slab);
+    for (int k = k0; k < k1; ++k, c += nxy) {
+        // this thread's copies of plane k+1 have landed; the barrier publishes everyone's
+        // copies of plane k and the slab of plane k, and frees the slot of plane k-1
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        __syncthreads();
+        issue(k + 3);
+        const unsigned u = (unsigned)(k - k0);
+        const PmvSlot<TZ>& S = slot[u % PMV_NS];
+        const double* P = slab + (u & 1u) * SLAB;
+        const double pt = form(slot[(u + 1) % PMV_NS], slab + ((u + 1) & 1u) * SLAB);
+        if (own) {
+            const double cxp = S.cx[ty][tx + 1], cxm = S.cx[ty][tx];
+            const double cyp = S.cy[ty + 1][tx], cym = S.cy[ty][tx];
+            const double czp = S.cz[ty][tx];
+            const double pw = P[fO - 1], pe = P[fO + 1], ps = P[fO - W], pn = P[fO + W];
+            double D = cxm + cxp + cym + cyp + czm + czp;
+            if (L.pin && c == 0) D += (nx > 1 ? cxp : 0.0) + (ny > 1 ? cyp : 0.0) + (nz > 1 ? czp : 0.0);
+            const double sum = cxp * pe + cxm * pw + cyp * pn + cym * ps + czp * pt + czm * pb;
+            const double y = (sum - D * pc) * L.inv_dx2;
+            Ap[c] = y;
+            pout[c] = pc;
+            acc += pc * y;
+            czm = czp;
+        }
+        pb = pc;
+        pc = pt;
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    double v[1] = {acc}, out[1];
+    if (grid_sums<PMV_TX * PMV_TY, 1>(v, partials, ticket, vb.count, out, vb.id)) st->pAp = out[0];
 }
 
 // x += alpha p; r -= alpha Ap (alpha = rho_new / pAp); ||r||^2 and, for the flexible form,
@@ -290,7 +479,10 @@ __global__ void __launch_bounds__(PK_NT) xr_update_kernel(size_t n, double* __re
                                                           const TZ* __restrict__ z, PcgState* st,
                                                           double* partials, unsigned* ticket,
                                                           cudaGraphConditionalHandle cond, int use_cond,
-                                                          float* __restrict__ r32) {
+                                                          float* __restrict__ r32, const double* p_alt) {
+    // p_alt: the second search-direction buffer of pmatvec_dot_kernel (p is then the first);
+    // this iteration's direction is the one that kernel wrote
+    if (p_alt) p = (st->iter & 1) ? p : p_alt;
     xr_update_body<TZ>(n, x, p, r, Ap, z, st, partials, ticket, cond, use_cond, r32, blockIdx.x, gridDim.x);
 }
 

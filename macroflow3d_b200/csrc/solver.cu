@@ -929,6 +929,7 @@ class HeadSolver {
         vec(b_);
         vec(r_);
         vec(p_);
+        vec(p2_);
         vec(Ap_);
         vec(x0_);
         // reduction scratch sized for the largest grid any reduction uses
@@ -1119,32 +1120,20 @@ class HeadSolver {
         const unsigned nb = grid1d(n, PK_NT);
         pcg_reopen_kernel<<<1, 1, 0, stream_>>>(st);
         MF3D_LAUNCH_CK();
-        out.push_back(timing("matvec_dot", tm.mean_ms(reps, [&] {
-            const ColLaunch cl = col_launch(G_[0].nx, G_[0].ny, G_[0].nz);
-            matvec_dot_kernel<double><<<cl.grid, cl.block, 0, stream_>>>(op64_[0], p_.as<double>(), Ap_.as<double>(),
-                                                                         st, partials_.as<double>(),
-                                                                         tickets_.as<unsigned>() + 3, cl.zchunk);
-            MF3D_LAUNCH_CK();
-        }), 40.0 * nd, 1));
+        out.push_back(timing("pupdate_matvec_dot", tm.mean_ms(reps, [&] { launch_pmatvec(stream_); }),
+                             (48.0 + ez) * nd, 1));
         out.push_back(timing("residual_true", tm.mean_ms(reps, [&] { launch_residual(stream_, 1); }), 48.0 * nd, 0));
-        out.push_back(timing("pupdate", tm.mean_ms(reps, [&] {
-            if (vc_->z_elt() == sizeof(double))
-                pupdate_kernel<double><<<nb, PK_NT, 0, stream_>>>(n, z_.as<double>(), p_.as<double>(), st);
-            else
-                pupdate_kernel<float><<<nb, PK_NT, 0, stream_>>>(n, z_.as<float>(), p_.as<double>(), st);
-            MF3D_LAUNCH_CK();
-        }), ez * nd + 16.0 * nd, 1));
         out.push_back(timing("xr_update", tm.mean_ms(reps, [&] {
             if (vc_->z_elt() == sizeof(double))
                 xr_update_kernel<double><<<nb, PK_NT, 0, stream_>>>(n, x_.as<double>(), p_.as<double>(), r_.as<double>(),
                                                                    Ap_.as<double>(), z_.as<double>(), st,
                                                                    partials_.as<double>(), tickets_.as<unsigned>() + 4,
-                                                                   cond_, 0, r32_.as<float>());
+                                                                   cond_, 0, r32_.as<float>(), p2_.as<double>());
             else
                 xr_update_kernel<float><<<nb, PK_NT, 0, stream_>>>(n, x_.as<double>(), p_.as<double>(), r_.as<double>(),
                                                                   Ap_.as<double>(), z_.as<float>(), st,
                                                                   partials_.as<double>(), tickets_.as<unsigned>() + 4,
-                                                                  cond_, 0, r32_.as<float>());
+                                                                  cond_, 0, r32_.as<float>(), p2_.as<double>());
             MF3D_LAUNCH_CK();
         }), 48.0 * nd + (flexible_ ? ez * nd : 0.0), 1));
         return out;
@@ -1153,6 +1142,31 @@ class HeadSolver {
     cudaStream_t stream() const { return stream_; }
 
   private:
+    // p = z + beta p fused with Ap = A p and <p, Ap> (z = r for plain CG)
+    void launch_pmatvec(cudaStream_t s) {
+        PcgState* st = state_.as<PcgState>();
+        const ColLaunch cl = col_launch(G_[0].nx, G_[0].ny, G_[0].nz, MF3D_PMATVEC_PERSM);
+        const bool z64 = cfg_.solver == MF3D_SOLVER_CG || vc_->z_elt() == sizeof(double);
+        // per call: the attribute belongs to the current device
+        if (z64)
+            MF3D_CK(cudaFuncSetAttribute(pmatvec_dot_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)pmv_smem_bytes<double>()));
+        else
+            MF3D_CK(cudaFuncSetAttribute(pmatvec_dot_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)pmv_smem_bytes<float>()));
+        if (z64) {
+            const double* z = cfg_.solver == MF3D_SOLVER_CG ? r_.as<double>() : z_.as<double>();
+            pmatvec_dot_kernel<double><<<cl.grid, cl.block, pmv_smem_bytes<double>(), s>>>(
+                op64_[0], z, p_.as<double>(), p2_.as<double>(), Ap_.as<double>(), st, partials_.as<double>(),
+                tickets_.as<unsigned>() + 3, cl.zchunk);
+        } else {
+            pmatvec_dot_kernel<float><<<cl.grid, cl.block, pmv_smem_bytes<float>(), s>>>(
+                op64_[0], z_.as<float>(), p_.as<double>(), p2_.as<double>(), Ap_.as<double>(), st,
+                partials_.as<double>(), tickets_.as<unsigned>() + 3, cl.zchunk);
+        }
+        MF3D_LAUNCH_CK();
+    }
+
     void launch_residual(cudaStream_t s, int mode) {
         const size_t n = G_[0].n;
         double* out = mode == 0 ? r_.as<double>() : Ap_.as<double>();
@@ -1188,31 +1202,18 @@ class HeadSolver {
         }
         const bool cg = cfg_.solver == MF3D_SOLVER_CG;
         if (!cg) vc_->run(s, z_.p, &st->rho_new);
-        if (cg || z64) {
-            const double* z = cg ? r_.as<double>() : z_.as<double>();
-            pupdate_kernel<double><<<nb, PK_NT, 0, s>>>(n, z, p_.as<double>(), st);
-        } else {
-            pupdate_kernel<float><<<nb, PK_NT, 0, s>>>(n, z_.as<float>(), p_.as<double>(), st);
-        }
-        MF3D_LAUNCH_CK();
-        {
-            const ColLaunch cl = col_launch(G_[0].nx, G_[0].ny, G_[0].nz);
-            matvec_dot_kernel<double><<<cl.grid, cl.block, 0, s>>>(op64_[0], p_.as<double>(), Ap_.as<double>(), st,
-                                                                   partials_.as<double>(), tickets_.as<unsigned>() + 3,
-                                                                   cl.zchunk);
-        }
-        MF3D_LAUNCH_CK();
+        launch_pmatvec(s);
         if (cg || z64) {
             const double* z = cg ? r_.as<double>() : z_.as<double>();
             xr_update_kernel<double><<<nb, PK_NT, 0, s>>>(n, x_.as<double>(), p_.as<double>(), r_.as<double>(),
                                                           Ap_.as<double>(), z, st, partials_.as<double>(),
                                                           tickets_.as<unsigned>() + 4, cond_, with_cond ? 1 : 0,
-                                                          r32_.as<float>());
+                                                          r32_.as<float>(), p2_.as<double>());
         } else {
             xr_update_kernel<float><<<nb, PK_NT, 0, s>>>(n, x_.as<double>(), p_.as<double>(), r_.as<double>(),
                                                          Ap_.as<double>(), z_.as<float>(), st, partials_.as<double>(),
                                                          tickets_.as<unsigned>() + 4, cond_, with_cond ? 1 : 0,
-                                                         r32_.as<float>());
+                                                         r32_.as<float>(), p2_.as<double>());
         }
         MF3D_LAUNCH_CK();
     }
@@ -1260,7 +1261,7 @@ class HeadSolver {
     std::vector<LevelOp<double>> op64_;
     std::vector<std::unique_ptr<CoefStore>> coef64_;
     std::vector<std::unique_ptr<DevMem>> Klev_;
-    DevMem x_, b_, r_, p_, Ap_, x0_, z_;
+    DevMem x_, b_, r_, p_, p2_, Ap_, x0_, z_; // p_, p2_: search directions, alternating by iteration
     DevMem partials_, tickets_, state_, mb_, err_, r32_;
     std::unique_ptr<VCycleBase> vc_;
     PcgState* host_state_ = nullptr;

@@ -307,3 +307,51 @@ def test_plain_cg_solver_vs_oracle(mf3d, oracle_mod):
     assert res.converged and ro.converged
     assert abs(res.num_iterations - ro.iterations) <= 2
     assert _rel(_np(h), ho) < 1e-7
+
+
+@pytest.mark.parametrize("case", BC_CASES, ids=[c[0] for c in BC_CASES])
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_pcg_every_bc_case_vs_oracle(mf3d, oracle_mod, case, prec):
+    """PCG (search-direction update fused with the matvec) on every boundary kind: periodic
+    wrap, the pinned cell, all-Dirichlet; 40 x 20 x 12 leaves partial column tiles in x and y
+    and halves evenly through the three levels (the CUDA hierarchy stops at an odd axis)."""
+    M, O = mf3d, oracle_mod
+    name, types, values, _ = case
+    shape = (12, 20, 40)
+    K = _lognormal(shape, 1.0, zlib.crc32(name.encode()))
+    g = M.Grid3D(shape[2], shape[1], shape[0], 1.0)
+    P = {"fp64": M.PREC_FP64, "fp32": M.PREC_FP32}[prec]
+    cfg = M.HeadSolveConfig(mg_levels=3, cg_rtol=1e-10, cg_check_every=1, precision=P)
+    # a random initial guess: with no Dirichlet face the right-hand side is zero, and the
+    # pinned system then iterates from x0 towards h = 0
+    x0 = np.random.default_rng(5).normal(size=shape)
+    s = M.HeadSolver(g, _bcs(M, types, values), cfg)
+    s.set_K(_t(K))
+    h = _t(np.zeros(shape))
+    res = s.solve(h, _t(x0))
+    ho, ro = O.solve_head_pcg(K, O.make_bc(types, values), 3, rtol=1e-10, check_every=1, h0=x0)
+    assert res.converged and ro.converged and ro.iterations > 3
+    if prec == "fp64":
+        assert abs(res.num_iterations - ro.iterations) <= 1
+    assert np.abs(_np(h) - ho).max() / max(np.abs(ho).max(), np.abs(x0).max()) < 1e-8
+    s.close()
+
+
+@pytest.mark.parametrize("case", BC_CASES, ids=[c[0] for c in BC_CASES])
+def test_plain_cg_every_bc_case_vs_oracle(mf3d, oracle_mod, case):
+    """Plain CG (z = r, the FP64 form of the fused update) on every boundary kind."""
+    M, O = mf3d, oracle_mod
+    name, types, values, _ = case
+    shape = (10, 18, 36)
+    K = _lognormal(shape, 0.5, zlib.crc32(("cg" + name).encode()))
+    g = M.Grid3D(shape[2], shape[1], shape[0], 1.0)
+    cfg = M.HeadSolveConfig(solver_type=M.SOLVER_CG, cg_max_iter=3000, cg_check_every=1, cg_rtol=1e-10)
+    s = M.HeadSolver(g, _bcs(M, types, values), cfg)
+    s.set_K(_t(K))
+    h = _t(np.zeros(shape))
+    res = s.solve(h)
+    ho, ro = O.solve_head_cg(K, O.make_bc(types, values), max_iter=3000, check_every=1, rtol=1e-10)
+    assert res.converged and ro.converged
+    assert abs(res.num_iterations - ro.iterations) <= 2
+    assert _rel(_np(h), ho) < 1e-7
+    s.close()
