@@ -26,6 +26,7 @@
 #include "kernels_kfield.cuh"
 #include "kernels_mg.cuh"
 #include "kernels_pcg.cuh"
+#include "kernels_resid.cuh"
 #include "kernels_setup.cuh"
 #include "kernels_sweep_tma.cuh"
 #include "kernels_tail.cuh"
@@ -496,8 +497,8 @@ template <class T, class TC> class VCycle : public VCycleBase {
                 int mode = (c ? 0 : M_ZERO) | (sw == pre_ ? M_RESID : 0);
                 rec_phase_ = 0;
                 rec_sw_ = sw;
-                // FP64 staged levels: the last pre-sweep, then the residual and its restriction
-                // in a kernel of their own (batched solves keep the fused form they record)
+                // staged levels: the last pre-sweep, then the residual and its restriction in a
+                // kernel of their own (batched solves keep the fused form they record)
                 const bool split = (mode & M_RESID) && tma_[l] && split_resid_ && !rec_;
                 sweep(s, l, c, out, nullptr, split ? nullptr : bc_next, split ? (mode & ~M_RESID) : mode, nullptr);
                 if (split) resid_restrict(s, l, out, bc_next);
@@ -794,13 +795,25 @@ template <class T, class TC> class VCycle : public VCycleBase {
 
     void resid_restrict(cudaStream_t s, int l, const T* x, T* out) {
         const Geom& g = G_[l];
-        const int gx = (g.nx / 2 + 31) / 32, gy = (g.ny / 2 + 7) / 8, ncz = g.nz / 2;
-        const long long cols = (long long)gx * gy;
-        const int nzc = (int)std::max<long long>(1, std::min<long long>(ncz, (long long)num_sms() * 8 / std::max(1LL, cols)));
-        const int zc = (ncz + nzc - 1) / nzc;
-        const dim3 grid(gx, gy, (ncz + zc - 1) / zc), block(32, 8);
         const T* b = l == 0 ? b0_ : (const T*)bl_[l]->p;
-        resid_restrict_kernel<T, TC><<<grid, block, 0, s>>>(ops_[l], x, b, out, zc);
+        if constexpr (sizeof(TC) >= 4) { // staged: 16 x 16 tiles, even z chunks
+            const int gx = (g.nx + RR_T - 1) / RR_T, gy = (g.ny + RR_T - 1) / RR_T, ncz = g.nz / 2;
+            const long long tiles = (long long)gx * gy;
+            const int nzc = (int)std::max<long long>(
+                1, std::min<long long>(ncz, (long long)num_sms() * MF3D_RR_PERSM / std::max(1LL, tiles)));
+            const int zc = 2 * ((ncz + nzc - 1) / nzc);
+            const dim3 grid(gx, gy, (g.nz + zc - 1) / zc);
+            MF3D_CK(cudaFuncSetAttribute(resid_restrict_staged_kernel<T, TC>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rr_smem_bytes<T, TC>()));
+            resid_restrict_staged_kernel<T, TC><<<grid, 256, rr_smem_bytes<T, TC>(), s>>>(ops_[l], x, b, out, zc);
+        } else {
+            const int gx = (g.nx / 2 + 31) / 32, gy = (g.ny / 2 + 7) / 8, ncz = g.nz / 2;
+            const long long cols = (long long)gx * gy;
+            const int nzc = (int)std::max<long long>(1, std::min<long long>(ncz, (long long)num_sms() * 8 / std::max(1LL, cols)));
+            const int zc = (ncz + nzc - 1) / nzc;
+            const dim3 grid(gx, gy, (ncz + zc - 1) / zc), block(32, 8);
+            resid_restrict_kernel<T, TC><<<grid, block, 0, s>>>(ops_[l], x, b, out, zc);
+        }
         MF3D_LAUNCH_CK();
     }
 
@@ -829,11 +842,12 @@ template <class T, class TC> class VCycle : public VCycleBase {
     std::vector<int> tma_;
     std::vector<std::array<Maps4, 2>> maps_;
     int n_tma_ = 0;
-    // FP64 staged levels: the residual and its restriction in a kernel of their own after the
-    // last pre-sweep, which computes every cell's residual exactly and is faster than the fused
-    // FP64 sweep (one CTA per SM); in FP32 the fused sweep is faster (measured at 256^3:
-    // 0.280 ms fused against 0.152 + 0.162 ms split)
-    static constexpr bool split_resid_ = sizeof(T) == 8;
+    // Staged levels with FP32 or FP64 coefficients: the residual and its restriction in a
+    // kernel of their own (resid_restrict_staged_kernel) after the last pre-sweep, which
+    // computes every cell's residual exactly and is faster than the fused RESID sweep
+    // (measured at 256^3 in FP32: 0.152 + 0.122 ms against 0.280 ms).  BF16 coefficients keep
+    // the fused sweep (cp.async moves at least 4 bytes).
+    static constexpr bool split_resid_ = sizeof(TC) >= 4;
     int occ_[16] = {}; // resident staged-sweep CTAs per SM, by mode
     std::unique_ptr<DevMem> tail_out_, tail_w_;
     Tail2Args tail_{};

@@ -17,6 +17,10 @@ HEAD_TOL = 1e-8
 # after a fixed number of iterations the iterates agree to rounding (the batch sums the
 # in-sweep <r, z> per work item, the single solve per CTA)
 ITERATE_TOL = 1e-10
+# ||r|| after six iterations (1e-5 of ||r0||) relative to each other: a single solve takes
+# the residual of the last pre-sweep in a kernel of its own, the batch inside the fused sweep,
+# and in FP32 the two round differently
+RESID_TOL = {"fp32": 1e-5, "fp64": 1e-6}
 # near the stopping threshold the plain FP64 method (Fletcher-Reeves beta with the reference's
 # non-symmetric V-cycle) converges unevenly, so a rounding difference can move the stop by an
 # iteration or two; the flexible mixed-precision method does not
@@ -102,7 +106,7 @@ def test_batch_iterates_match_single_solves(mf3d, prec):
     for (hr, rr), (hb, rb) in zip(ref, got):
         assert rr.num_iterations == rb.num_iterations == 6 and not rb.converged
         assert _rel(hb, hr) < ITERATE_TOL
-        assert abs(rb.final_residual - rr.final_residual) <= 1e-6 * rr.final_residual
+        assert abs(rb.final_residual - rr.final_residual) <= RESID_TOL[prec] * rr.final_residual
     b.close()
 
 
