@@ -214,7 +214,7 @@ __device__ __forceinline__ void matvec_dot_body(const LevelOp<TC>& L, const doub
 // 2.5-D blocking: a CTA of 32 x 8 threads owns a 32 x 8 column tile and marches a z chunk.
 // Every thread stages, by cp.async into a ring of PMV_NS shared-memory slots, the z and p_old
 // of its own cell (and of the ring cells beside the tile that it is assigned) and its cell's
-// +x/+y/+z faces (the threads on the -x/-y edges also the -x/-y faces), three planes ahead of
+// +x/+y/+z faces (the threads on the -x/-y edges also the -x/-y faces), PMV_NS - 1 planes ahead of
 // the plane it applies: those copies are in flight while the CTA computes.  From a landed
 // slot each thread forms p_new of the cells it staged into a double-buffered slab (tile plus
 // one-cell ring); the stencil reads its x/y neighbours from the slab, its -z/+z values and
@@ -232,7 +232,10 @@ __device__ __forceinline__ double* pcg_pbuf_out(int iter, double* p0, double* p1
 #ifndef MF3D_PMATVEC_PERSM
 #define MF3D_PMATVEC_PERSM 8 // CTAs launched per SM (z chunks sized to match)
 #endif
-constexpr int PMV_TX = 32, PMV_TY = 8, PMV_NS = 4;
+#ifndef MF3D_PMATVEC_NS
+#define MF3D_PMATVEC_NS 4 // staged planes: the one applied, the next, PMV_NS - 2 in flight
+#endif
+constexpr int PMV_TX = 32, PMV_TY = 8, PMV_NS = MF3D_PMATVEC_NS;
 
 template <class TZ> struct PmvSlot {
     TZ z[PMV_TY + 2][PMV_TX + 2];     // tile and ring, row 0 / column 0 at j0-1 / i0-1
@@ -369,17 +372,16 @@ __global__ void __launch_bounds__(PMV_TX * PMV_TY, MF3D_PMATVEC_MINB)
         czm = k0 > 0 ? __ldg(L.cz + c - nxy)
                      : (L.per_z ? __ldg(L.cz + c + (size_t)(nz - 1) * nxy) : __ldg(L.bzm + cO));
     }
-    issue(k0);
-    issue(k0 + 1);
-    issue(k0 + 2);
-    asm volatile("cp.async.wait_group 2;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < PMV_NS - 1; ++q) issue(k0 + q);
+    asm volatile("cp.async.wait_group %0;" ::"n"(PMV_NS - 2) : "memory");
     double pc = form(slot[0], slab);
     for (int k = k0; k < k1; ++k, c += nxy) {
         // this thread's copies of plane k+1 have landed; the barrier publishes everyone's
         // copies of plane k and the slab of plane k, and frees the slot of plane k-1
-        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        asm volatile("cp.async.wait_group %0;" ::"n"(PMV_NS - 3) : "memory");
         __syncthreads();
-        issue(k + 3);
+        issue(k + PMV_NS - 1);
         const unsigned u = (unsigned)(k - k0);
         const PmvSlot<TZ>& S = slot[u % PMV_NS];
         const double* P = slab + (u & 1u) * SLAB;

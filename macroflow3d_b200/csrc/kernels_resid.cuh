@@ -7,7 +7,7 @@
 //
 // 2.5-D blocking as in pmatvec_dot_kernel (kernels_pcg.cuh): a CTA of 256 threads owns a
 // 16 x 16 column tile and marches an even z chunk; each thread stages, by cp.async into a ring
-// of RR_NS shared-memory slots, its own cell's x, b and +x/+y/+z faces three planes ahead, and
+// of RR_NS shared-memory slots, its own cell's x, b and +x/+y/+z faces RR_NS - 1 planes ahead, and
 // three warps stage the tile's x ring and its -x/-y faces.  A warp covers two rows of 16
 // cells, so the 2 x 2 children of a coarse cell in a plane are summed by two shuffles and the
 // two planes of a coarse cell in a register.  x of the plane below and the -z face are
@@ -26,7 +26,10 @@ namespace mf3d {
 #ifndef MF3D_RR_PERSM
 #define MF3D_RR_PERSM 8 // CTAs launched per SM (z chunks sized to match)
 #endif
-constexpr int RR_T = 16, RR_NS = 4;
+#ifndef MF3D_RR_NS
+#define MF3D_RR_NS 4 // staged planes: the one applied, the next, RR_NS - 2 in flight
+#endif
+constexpr int RR_T = 16, RR_NS = MF3D_RR_NS;
 
 template <class T, class TC> struct RrSlot {
     T x[RR_T + 2][RR_T + 2];  // tile and its one-cell ring
@@ -135,16 +138,15 @@ __global__ void __launch_bounds__(256, MF3D_RR_MINB)
     }
     const bool writer = own && !(tx & 1) && !(ty & 1);
     const size_t cc0 = (size_t)(i >> 1) + (size_t)ncx * (size_t)(j >> 1);
-    issue(k0);
-    issue(k0 + 1);
-    issue(k0 + 2);
+#pragma unroll
+    for (int q = 0; q < RR_NS - 1; ++q) issue(k0 + q);
     T accz = (T)0;
     for (int k = k0; k < k1; ++k, c += nxy) {
         // this thread's copies of plane k+1 have landed; the barrier publishes everyone's
         // copies of plane k and frees the slot of plane k-1
-        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        asm volatile("cp.async.wait_group %0;" ::"n"(RR_NS - 3) : "memory");
         __syncthreads();
-        issue(k + 3);
+        issue(k + RR_NS - 1);
         const unsigned u = (unsigned)(k - k0);
         const RrSlot<T, TC>& S = slot[u % RR_NS];
         const T* X = &S.x[0][0];
