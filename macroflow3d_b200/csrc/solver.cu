@@ -796,8 +796,8 @@ template <class T, class TC> class VCycle : public VCycleBase {
     void resid_restrict(cudaStream_t s, int l, const T* x, T* out) {
         const Geom& g = G_[l];
         const T* b = l == 0 ? b0_ : (const T*)bl_[l]->p;
-        if constexpr (sizeof(TC) >= 4) { // staged: 16 x 16 tiles, even z chunks
-            const int gx = (g.nx + RR_T - 1) / RR_T, gy = (g.ny + RR_T - 1) / RR_T, ncz = g.nz / 2;
+        if constexpr (sizeof(TC) >= 4) { // staged: 32 x 16 tiles of x-pairs, even z chunks
+            const int gx = (g.nx + RR_TX - 1) / RR_TX, gy = (g.ny + RR_TY - 1) / RR_TY, ncz = g.nz / 2;
             const long long tiles = (long long)gx * gy;
             const int nzc = (int)std::max<long long>(
                 1, std::min<long long>(ncz, (long long)num_sms() * MF3D_RR_PERSM / std::max(1LL, tiles)));
