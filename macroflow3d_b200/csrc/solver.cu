@@ -845,7 +845,7 @@ template <class T, class TC> class VCycle : public VCycleBase {
     // Staged levels with FP32 or FP64 coefficients: the residual and its restriction in a
     // kernel of their own (resid_restrict_staged_kernel) after the last pre-sweep, which
     // computes every cell's residual exactly and is faster than the fused RESID sweep
-    // (measured at 256^3 in FP32: 0.152 + 0.122 ms against 0.280 ms).  BF16 coefficients keep
+    // (measured at 256^3 in FP32: 0.152 + 0.069 ms against 0.280 ms).  BF16 coefficients keep
     // the fused sweep (cp.async moves at least 4 bytes).
     static constexpr bool split_resid_ = sizeof(TC) >= 4;
     int occ_[16] = {}; // resident staged-sweep CTAs per SM, by mode
