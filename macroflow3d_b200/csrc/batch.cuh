@@ -183,6 +183,7 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
                 it.b = H.b_.as<double>();
                 it.r = H.r_.as<double>();
                 it.p = H.p_.as<double>();
+                it.p2 = H.p2_.as<double>();
                 it.Ap = H.Ap_.as<double>();
                 it.z = H.z_.p;
                 it.r32 = H.r32_.as<float>();
@@ -551,9 +552,10 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
     void record_body(cudaStream_t s, bool with_cond) {
         const int R = (int)hs_.size();
         record_vcycle(s);
-        batch_pupdate_kernel<T><<<pgrid(tot1_), PK_NT, 0, s>>>(items_d_, off1_d_, R, tot1_);
-        MF3D_LAUNCH_CK();
-        batch_matvec_dot_kernel<<<pgrid(tot3_), dim3(32, 8), 0, s>>>(items_d_, off3_d_, R, tot3_);
+        MF3D_CK(cudaFuncSetAttribute(batch_pmatvec_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)pmv_smem_bytes<T>()));
+        batch_pmatvec_kernel<T><<<pgrid(tot3_), dim3(PMV_TX, PMV_TY), pmv_smem_bytes<T>(), s>>>(items_d_, off3_d_, R,
+                                                                                             tot3_);
         MF3D_LAUNCH_CK();
         batch_xr_update_kernel<T><<<pgrid(tot1_), PK_NT, 0, s>>>(items_d_, off1_d_, R, tot1_);
         MF3D_LAUNCH_CK();

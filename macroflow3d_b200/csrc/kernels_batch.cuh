@@ -18,7 +18,8 @@ struct PcgItem {
     double* x;
     const double* b;
     double* r;
-    double* p;
+    double* p;  // search directions: p and p2 alternate by iteration (pmatvec_body)
+    double* p2;
     double* Ap;
     const void* z;  // preconditioned residual, the V-cycle's type
     float* r32;     // FP32 copy of r for a mixed-precision V-cycle, or null
@@ -124,26 +125,18 @@ __global__ void __launch_bounds__(PK_NT) batch_residual_kernel(const PcgItem* __
     }
 }
 
+// p = z + beta p, Ap = A p and <p, Ap> (pmatvec_body) for every running realisation; dynamic
+// shared memory pmv_smem_bytes<TZ>()
 template <class TZ>
-__global__ void __launch_bounds__(PK_NT) batch_pupdate_kernel(const PcgItem* __restrict__ items,
-                                                              const int* __restrict__ off, int nseg, int total) {
+__global__ void __launch_bounds__(PMV_TX * PMV_TY, MF3D_PMATVEC_MINB)
+    batch_pmatvec_kernel(const PcgItem* __restrict__ items, const int* __restrict__ off, int nseg, int total) {
+    extern __shared__ __align__(16) unsigned char bpmv_sm[];
     for (int b = blockIdx.x; b < total; b += gridDim.x) {
         const int s = find_seg(off, nseg, b);
         const PcgItem& it = items[s];
-        if (it.st->stop) continue;
-        const int o = __ldg(off + s);
-        pupdate_body<TZ>(it.n, (const TZ*)it.z, it.p, it.st, b - o, __ldg(off + s + 1) - o);
-    }
-}
-
-__global__ void __launch_bounds__(PK_NT) batch_matvec_dot_kernel(const PcgItem* __restrict__ items,
-                                                                 const int* __restrict__ off, int nseg, int total) {
-    for (int b = blockIdx.x; b < total; b += gridDim.x) {
-        const int s = find_seg(off, nseg, b);
-        const PcgItem& it = items[s];
-        if (it.st->stop) continue;
         const VBlk vb = make_vblk(b - __ldg(off + s), it.cgx, it.cgy, it.cgz);
-        matvec_dot_body<double>(it.L, it.p, it.Ap, it.st, it.partials, it.tickets + 3, it.zchunk, vb);
+        pmatvec_body<TZ>(it.L, (const TZ*)it.z, it.p, it.p2, it.Ap, it.st, it.partials, it.tickets + 3, it.zchunk, vb,
+                         bpmv_sm);
     }
 }
 
@@ -155,7 +148,8 @@ __global__ void __launch_bounds__(PK_NT) batch_xr_update_kernel(const PcgItem* _
         const PcgItem& it = items[s];
         if (it.st->stop) continue;
         const int o = __ldg(off + s);
-        xr_update_body<TZ>(it.n, it.x, it.p, it.r, it.Ap, (const TZ*)it.z, it.st, it.partials, it.tickets + 4, 0, 0,
+        const double* p = pcg_pbuf_out(it.st->iter, it.p, it.p2); // this iteration's direction
+        xr_update_body<TZ>(it.n, it.x, p, it.r, it.Ap, (const TZ*)it.z, it.st, it.partials, it.tickets + 4, 0, 0,
                            it.r32, b - o, __ldg(off + s + 1) - o);
     }
 }

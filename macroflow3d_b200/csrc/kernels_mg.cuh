@@ -232,43 +232,6 @@ __global__ void __launch_bounds__(SW_NT) sweep_batch_kernel(const SweepArgs<T, T
     sweep_body<T, TC, TB, MODE>(a, make_vblk(blockIdx.x - off[s], d.x, d.y, d.z));
 }
 
-// r = b - A x on a fine level with the smoother's pin convention (diagonal doubled at cell 0;
-// compute_residual_3d, src/multigrid/smoothers/residual_3d.cu:365-368) and its 8-cell average
-// into the coarse right-hand side (restrict_3d.cu:38-49 order: children 000, 100, 010, 110,
-// 001, 101, 011, 111), without a residual array.  One thread per coarse column (I, J)
-// marching the coarse planes of its chunk.  Non-periodic levels: a neighbour outside the grid
-// is 0 and its face coefficient comes from the boundary planes.
-template <class T, class TC>
-__global__ void __launch_bounds__(256) resid_restrict_kernel(const LevelOp<TC> L, const T* __restrict__ x,
-                                                             const T* __restrict__ b, T* __restrict__ b_coarse,
-                                                             int zchunk) {
-    const int ncx = L.nx >> 1, ncy = L.ny >> 1, ncz = L.nz >> 1;
-    const int I = blockIdx.x * 32 + threadIdx.x, J = blockIdx.y * 8 + threadIdx.y;
-    if (I >= ncx || J >= ncy) return;
-    const int nx = L.nx, ny = L.ny, nz = L.nz;
-    const size_t nxy = (size_t)nx * ny;
-    const T inv_dx2 = (T)L.inv_dx2;
-    const int K0 = blockIdx.z * zchunk, K1 = min(ncz, K0 + zchunk);
-    for (int K = K0; K < K1; ++K) {
-        T acc = (T)0;
-#pragma unroll
-        for (int d = 0; d < 8; ++d) {
-            const int i = 2 * I + (d & 1), j = 2 * J + ((d >> 1) & 1), k = 2 * K + (d >> 2);
-            const size_t c = (size_t)i + (size_t)nx * j + nxy * k;
-            T cxm, cxp, cym, cyp, czm, czp;
-            cell_coefs<T>(L, i, j, k, c, cxm, cxp, cym, cyp, czm, czp);
-            T D = cxm + cxp + cym + cyp + czm + czp;
-            if (L.pin && c == 0) D *= (T)2;
-            const T xw = i > 0 ? __ldg(x + c - 1) : (T)0, xe = i < nx - 1 ? __ldg(x + c + 1) : (T)0;
-            const T xs = j > 0 ? __ldg(x + c - nx) : (T)0, xn = j < ny - 1 ? __ldg(x + c + nx) : (T)0;
-            const T xb = k > 0 ? __ldg(x + c - nxy) : (T)0, xt = k < nz - 1 ? __ldg(x + c + nxy) : (T)0;
-            const T sum = cxp * xe + cxm * xw + cyp * xn + cym * xs + czp * xt + czm * xb;
-            acc += __ldg(b + c) - (sum - D * __ldg(x + c)) * inv_dx2;
-        }
-        b_coarse[(size_t)I + (size_t)ncx * ((size_t)J + (size_t)ncy * K)] = acc / (T)8;
-    }
-}
-
 // x_out = x_in + P e_c  (or P e_c when x_in is null): the prolongation alone, for levels
 // configured with zero post-smoothing sweeps.
 template <class T>

@@ -168,48 +168,12 @@ __global__ void __launch_bounds__(PK_NT) residual_kernel(const LevelOp<TC> L, co
     residual_body<TC>(L, x, b, r, st, partials, ticket, mode, ref_is_b, r32, cond, use_cond, zchunk, hw_vblk());
 }
 
-// p = z + beta p; beta = 0 on the first iteration, Fletcher-Reeves rho_new/rho_old, or the
-// flexible Polak-Ribiere form (rho_new - gamma)/rho_old.
-template <class TZ>
-__device__ __forceinline__ void pupdate_body(size_t n, const TZ* __restrict__ z, double* __restrict__ p, PcgState* st,
-                                             int blk, int nblk) {
-    const PcgState s = *st;
-    if (s.stop) return;
-    const double beta = s.iter == 0 ? 0.0 : (s.rho_new - (s.flexible ? s.gamma : 0.0)) / s.rho_old;
-    if (blk == 0 && threadIdx.x == 0) st->beta = beta;
-    if (s.iter == 0) { // p = z exactly: whatever p held before must not leak in through 0 * p
-        for (size_t c = blk * (size_t)PK_NT + threadIdx.x; c < n; c += (size_t)nblk * PK_NT) p[c] = (double)z[c];
-        return;
-    }
-    for (size_t c = blk * (size_t)PK_NT + threadIdx.x; c < n; c += (size_t)nblk * PK_NT)
-        p[c] = 1.0 * (double)z[c] + beta * p[c];
-}
-
-// Ap = A p and <p, Ap>.
-template <class TC>
-__device__ __forceinline__ void matvec_dot_body(const LevelOp<TC>& L, const double* __restrict__ p,
-                                                double* __restrict__ Ap, PcgState* st, double* partials,
-                                                unsigned* ticket, int zchunk, const VBlk& vb) {
-    if (st->stop) return;
-    double acc = 0.0;
-    const Col3 q = col3(L.nx, L.ny, L.nz, zchunk, vb.x, vb.y, vb.z);
-    if (q.ok) {
-        const size_t nxy = (size_t)L.nx * L.ny;
-        for (int k = q.k0; k < q.k1; ++k) {
-            const size_t c = (size_t)q.i + (size_t)L.nx * q.j + nxy * k;
-            const double y = apply_A_cell(L, p, q.i, q.j, k, c);
-            Ap[c] = y;
-            acc += __ldg(p + c) * y;
-        }
-    }
-    double v[1] = {acc}, out[1];
-    if (grid_sums<PK_NT, 1>(v, partials, ticket, vb.count, out, vb.id)) st->pAp = out[0];
-}
-
-// The search-direction update of pupdate_body fused with matvec_dot_body: p_new = z + beta
-// p_old is formed once per cell from z and p_old and written once, instead of written by one
-// kernel and re-read by the next.  p_old and p_new live in two buffers that swap by iteration
-// parity (pcg_pbuf_in / pcg_pbuf_out): no CTA overwrites a value that another still reads.
+// The search-direction update p = z + beta p (beta = 0 on the first iteration, where p = z
+// exactly; Fletcher-Reeves rho_new / rho_old, or the flexible Polak-Ribiere form
+// (rho_new - gamma) / rho_old) fused with Ap = A p and <p, Ap>: p_new is formed once per cell
+// from z and p_old and written once, instead of written by one kernel and re-read by the
+// next.  p_old and p_new live in two buffers that swap by iteration parity (pcg_pbuf_in /
+// pcg_pbuf_out): no CTA overwrites a value that another still reads.
 //
 // 2.5-D blocking: a CTA of 32 x 8 threads owns a 32 x 8 column tile and marches a z chunk.
 // Every thread stages, by cp.async into a ring of PMV_NS shared-memory slots, the z and p_old
@@ -219,8 +183,8 @@ __device__ __forceinline__ void matvec_dot_body(const LevelOp<TC>& L, const doub
 // slot each thread forms p_new of the cells it staged into a double-buffered slab (tile plus
 // one-cell ring); the stencil reads its x/y neighbours from the slab, its -z/+z values and
 // its -z face from registers.  One barrier per plane.  Cells outside a non-periodic axis are
-// staged as zeros (the operator's ghost value, p_new = 0); periodic axes wrap.  Arithmetic
-// per cell is that of pupdate_body and apply_A_cell, bit for bit.
+// staged as zeros (the operator's ghost value, p_new = 0); periodic axes wrap.  The stencil
+// arithmetic per cell is that of apply_A_cell.
 __device__ __forceinline__ const double* pcg_pbuf_in(int iter, const double* p0, const double* p1) {
     return (iter & 1) ? p1 : p0;
 }
@@ -255,19 +219,22 @@ template <int B> __device__ __forceinline__ void pmv_cp(void* dst, const void* s
                  : "memory");
 }
 
+// One virtual block (32 x 8 column tile, one z chunk) of one realisation; `sm` is the CTA's
+// dynamic shared memory (pmv_smem_bytes<TZ>()).  Every thread of the CTA calls it with the
+// same arguments; a CTA that runs several blocks in turn separates them with the barrier at
+// the top.
 template <class TZ>
-__global__ void __launch_bounds__(PMV_TX * PMV_TY, MF3D_PMATVEC_MINB)
-    pmatvec_dot_kernel(const LevelOp<double> L, const TZ* __restrict__ z, double* p0, double* p1,
-                       double* __restrict__ Ap, PcgState* st, double* partials, unsigned* ticket, int zchunk) {
+__device__ __forceinline__ void pmatvec_body(const LevelOp<double>& L, const TZ* __restrict__ z, double* p0,
+                                             double* p1, double* __restrict__ Ap, PcgState* st, double* partials,
+                                             unsigned* ticket, int zchunk, const VBlk& vb, unsigned char* sm) {
     constexpr int W = PMV_TX + 2; // slab / staged-plane row pitch
-    extern __shared__ __align__(16) unsigned char pmv_sm[];
-    PmvSlot<TZ>* slot = reinterpret_cast<PmvSlot<TZ>*>(pmv_sm);
-    double* slab = reinterpret_cast<double*>(pmv_sm + PMV_NS * sizeof(PmvSlot<TZ>)); // [2][PMV_TY + 2][W]
+    PmvSlot<TZ>* slot = reinterpret_cast<PmvSlot<TZ>*>(sm);
+    double* slab = reinterpret_cast<double*>(sm + PMV_NS * sizeof(PmvSlot<TZ>)); // [2][PMV_TY + 2][W]
+    __syncthreads(); // the previous block's reads of the slots and the slab are done
     const PcgState s = *st;
     if (s.stop) return;
     const bool first = s.iter == 0;
     const double beta = first ? 0.0 : (s.rho_new - (s.flexible ? s.gamma : 0.0)) / s.rho_old;
-    const VBlk vb = hw_vblk();
     const int tx = threadIdx.x, ty = threadIdx.y;
     if (vb.id == 0 && tx == 0 && ty == 0) st->beta = beta;
     const double* __restrict__ pin = pcg_pbuf_in(s.iter, p0, p1);
@@ -406,6 +373,14 @@ __global__ void __launch_bounds__(PMV_TX * PMV_TY, MF3D_PMATVEC_MINB)
     asm volatile("cp.async.wait_all;" ::: "memory");
     double v[1] = {acc}, out[1];
     if (grid_sums<PMV_TX * PMV_TY, 1>(v, partials, ticket, vb.count, out, vb.id)) st->pAp = out[0];
+}
+
+template <class TZ>
+__global__ void __launch_bounds__(PMV_TX * PMV_TY, MF3D_PMATVEC_MINB)
+    pmatvec_dot_kernel(const LevelOp<double> L, const TZ* __restrict__ z, double* p0, double* p1,
+                       double* __restrict__ Ap, PcgState* st, double* partials, unsigned* ticket, int zchunk) {
+    extern __shared__ __align__(16) unsigned char pmv_sm[];
+    pmatvec_body<TZ>(L, z, p0, p1, Ap, st, partials, ticket, zchunk, hw_vblk(), pmv_sm);
 }
 
 // x += alpha p; r -= alpha Ap (alpha = rho_new / pAp); ||r||^2 and, for the flexible form,

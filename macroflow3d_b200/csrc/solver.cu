@@ -806,15 +806,10 @@ template <class T, class TC> class VCycle : public VCycleBase {
             MF3D_CK(cudaFuncSetAttribute(resid_restrict_staged_kernel<T, TC>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rr_smem_bytes<T, TC>()));
             resid_restrict_staged_kernel<T, TC><<<grid, 256, rr_smem_bytes<T, TC>(), s>>>(ops_[l], x, b, out, zc);
+            MF3D_LAUNCH_CK();
         } else {
-            const int gx = (g.nx / 2 + 31) / 32, gy = (g.ny / 2 + 7) / 8, ncz = g.nz / 2;
-            const long long cols = (long long)gx * gy;
-            const int nzc = (int)std::max<long long>(1, std::min<long long>(ncz, (long long)num_sms() * 8 / std::max(1LL, cols)));
-            const int zc = (ncz + nzc - 1) / nzc;
-            const dim3 grid(gx, gy, (ncz + zc - 1) / zc), block(32, 8);
-            resid_restrict_kernel<T, TC><<<grid, block, 0, s>>>(ops_[l], x, b, out, zc);
+            throw Error(MF3D_E_INVALID, "the separate residual kernel needs 4- or 8-byte coefficients");
         }
-        MF3D_LAUNCH_CK();
     }
 
     void restrict_b(cudaStream_t s, int l, T* out) {
