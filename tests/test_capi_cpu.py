@@ -160,3 +160,13 @@ def test_flow_yaml_strict_keys(mf3d):
     # defaults of FlowYamlConfig (Config.hpp:86-114)
     d = mf3d.load_flow_yaml("flow: {}\n")
     assert d.solver == "mg" and d.cg_max_iter == 1000 and d.bc.types == (0,) * 6
+
+
+def test_solve_once_cli_parses_without_a_gpu():
+    """The single-solve CLI used for kernel captures parses its options before any device work."""
+    import subprocess
+    import sys
+    out = subprocess.run([sys.executable, "-m", "macroflow3d_b200.solve_once", "--help"], capture_output=True,
+                         text=True, timeout=120, cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    assert out.returncode == 0, out.stderr
+    assert "--precision" in out.stdout and "--graph" in out.stdout
