@@ -2,6 +2,8 @@
 // reference's C++ head-solver interface (santi-esquerre/MacroFlow3D):
 //
 //   mf3d::HeadSolveConfig / HeadSolveResult    src/physics/flow/solve_head.cuh:63-141
+//   mf3d::FlowYamlConfig, HeadSolveConfig::from_yaml   src/io/config/Config.hpp:86-114,
+//                                                      solve_head.cuh:98-130
 //   mf3d::FlowWorkspace                         src/physics/common/workspaces.cuh:111-167
 //   mf3d::solve_head(h, K, grid, bc, cfg, ctx, ws)                solve_head.cuh:158-160
 //   mf3d::compute_velocity_from_head(U, V, W, layout, h, K, ...)  velocity_from_head.cuh:54-73
@@ -40,9 +42,50 @@ struct BCSpec {
     }
 };
 
+// PinMode (src/numerics/pin_spec.hpp:56-60).
+enum class PinMode { Auto = MF3D_PIN_AUTO, On = MF3D_PIN_ON, Off = MF3D_PIN_OFF };
+
+// The `flow:` section of the reference's YAML configuration after parsing
+// (src/io/config/Config.hpp:86-114): a caller that parses its YAML with the reference's
+// ConfigYaml keeps doing so and copies the fields here, or fills them directly.
+struct FlowYamlConfig {
+    std::string solver = "mg"; // "mg", "cg", "mg_cg" / "pcg_mg"
+    int mg_levels = 4;
+    int mg_pre_smooth = 2;
+    int mg_post_smooth = 2;
+    int mg_coarse_iters = 50;
+    int mg_max_cycles = 20;
+    int cg_max_iter = 1000;
+    double cg_rtol = 1e-8;
+    int cg_check_every = 10;
+    double rtol = 1e-6;
+    BCSpec bc = BCSpec::darcy_x();
+    PinMode pin = PinMode::Auto;
+};
+
 struct HeadSolveConfig {
     mf3d_solver_config cfg{};
     HeadSolveConfig() { check(mf3d_default_config(&cfg)); }
+
+    // HeadSolveConfig::from_yaml (src/physics/flow/solve_head.cuh:98-130): the solver string
+    // maps to the solver type, unknown strings to PCG_MG; every numeric field is copied.
+    static HeadSolveConfig from_yaml(const FlowYamlConfig& f) {
+        HeadSolveConfig c;
+        if (f.solver == "cg") c.cfg.solver = MF3D_SOLVER_CG;
+        else if (f.solver == "mg") c.cfg.solver = MF3D_SOLVER_MG;
+        else c.cfg.solver = MF3D_SOLVER_PCG_MG;
+        c.cfg.mg_levels = f.mg_levels;
+        c.cfg.mg_pre_smooth = f.mg_pre_smooth;
+        c.cfg.mg_post_smooth = f.mg_post_smooth;
+        c.cfg.mg_max_cycles = f.mg_max_cycles;
+        c.cfg.mg_coarse_iters = f.mg_coarse_iters;
+        c.cfg.cg_max_iter = f.cg_max_iter;
+        c.cfg.cg_rtol = f.cg_rtol;
+        c.cfg.cg_check_every = f.cg_check_every;
+        c.cfg.rtol = f.rtol;
+        c.cfg.pin_mode = (int)f.pin;
+        return c;
+    }
 };
 
 struct HeadSolveResult {
@@ -53,7 +96,10 @@ struct HeadSolveResult {
     mf3d_solve_result raw{};
 };
 
-// Owns the solver of one grid; rebuilt when the grid changes (solve_head.cu:89-94).
+// Owns the solver of one problem.  The reference rebuilds its hierarchy when the grid changes
+// (solve_head.cu:89-94) and takes the BCs and the configuration on every call
+// (solve_head.cuh:158-160); the solver here bakes the grid, BCs, configuration and stream into
+// its operator and CUDA graph, so it is re-created when any of them differs from the last call.
 class FlowWorkspace {
   public:
     FlowWorkspace() = default;
@@ -65,19 +111,44 @@ class FlowWorkspace {
         s_ = nullptr;
     }
     mf3d_head_solver* ensure(const Grid3D& g, const BCSpec& bc, const HeadSolveConfig& c, void* stream) {
-        if (!s_ || g.nx != g_.nx || g.ny != g_.ny || g.nz != g_.nz || g.dx != g_.dx) {
+        const bool same = s_ && g.nx == g_.nx && g.ny == g_.ny && g.nz == g_.nz && g.dx == g_.dx &&
+                          same_bc(bc.bc, bc_.bc) && same_cfg(c.cfg, cfg_.cfg) && stream == stream_;
+        if (!same) {
             reset();
             mf3d_grid gc = g.c();
             check(mf3d_head_solver_create(&gc, &bc.bc, &c.cfg, stream, &s_));
             g_ = g;
+            bc_ = bc;
+            cfg_ = c;
+            stream_ = stream;
+            ++builds_;
         }
         return s_;
     }
     mf3d_head_solver* get() const { return s_; }
+    // how many times a solver was created (diagnostics)
+    int builds() const { return builds_; }
 
   private:
+    static bool same_bc(const mf3d_bc& a, const mf3d_bc& b) {
+        for (int f = 0; f < 6; ++f)
+            if (a.type[f] != b.type[f] || a.value[f] != b.value[f]) return false;
+        return true;
+    }
+    static bool same_cfg(const mf3d_solver_config& a, const mf3d_solver_config& b) {
+        return a.solver == b.solver && a.mg_levels == b.mg_levels && a.mg_pre_smooth == b.mg_pre_smooth &&
+               a.mg_post_smooth == b.mg_post_smooth && a.mg_max_cycles == b.mg_max_cycles &&
+               a.mg_coarse_iters == b.mg_coarse_iters && a.cg_max_iter == b.cg_max_iter &&
+               a.cg_check_every == b.cg_check_every && a.cg_rtol == b.cg_rtol && a.rtol == b.rtol &&
+               a.pin_mode == b.pin_mode && a.precision == b.precision && a.flexible == b.flexible &&
+               a.conv_norm == b.conv_norm && a.use_graph == b.use_graph;
+    }
     mf3d_head_solver* s_ = nullptr;
     Grid3D g_;
+    BCSpec bc_;
+    HeadSolveConfig cfg_;
+    void* stream_ = nullptr;
+    int builds_ = 0;
 };
 
 // solve_head: h (device, out), K (device), the reference's arguments; `stream` is the

@@ -760,3 +760,140 @@ void og_lnk_eval(int nx, int ny, int nz, double dx, int n_modes, const double* k
                 lnk[IX(i, j, k)] = scale * s;
             }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Randomization-method modes on the host, and lnK evaluated in x-runs.       */
+/*                                                                            */
+/* The reference draws its modes with cuRAND XORWOW (stochastic.cu:43-91) and */
+/* is isotropic; the product draws them with Philox4x32-10 (Salmon, Moraes,   */
+/* Dror, Shaw, SC'11), counter (mode, draw, 0, 0), key = seed, and divides    */
+/* each wavenumber component by its own correlation length.  This is a        */
+/* restatement of that published sampler so that a process that must not load */
+/* the product (the reference arm of the bench) can build the same K field.   */
+/* The wavenumber magnitude follows stochastic.cu:70-83 (exponential:         */
+/* half-Cauchy proposal accepted with k^2/(1+k^2)) and :118-160 (Gaussian).   */
+/* ------------------------------------------------------------------------ */
+static void og_philox(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t out[4]) {
+    uint32_t c[4] = {c0, c1, 0u, 0u};
+    uint32_t k[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k[0];
+        const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k[1];
+        c[1] = (uint32_t)p1;
+        c[3] = (uint32_t)p0;
+        c[0] = n0;
+        c[2] = n2;
+        k[0] += 0x9E3779B9u;
+        k[1] += 0xBB67AE85u;
+    }
+    memcpy(out, c, sizeof c);
+}
+
+typedef struct {
+    uint64_t seed;
+    uint32_t mode, draw;
+    uint32_t buf[4];
+    int have;
+} og_mode_rng;
+
+/* 53 random bits from two words, as a double strictly inside (0, 1) */
+static double og_u01(og_mode_rng* g) {
+    if (g->have == 0) {
+        og_philox(g->seed, g->mode, g->draw++, g->buf);
+        g->have = 2;
+    }
+    const uint32_t a = g->have == 2 ? g->buf[0] : g->buf[2];
+    const uint32_t b = g->have == 2 ? g->buf[1] : g->buf[3];
+    --g->have;
+    const uint64_t v = ((uint64_t)(a >> 5) << 26) | (uint64_t)(b >> 6);
+    return ((double)v + 0.5) / 9007199254740992.0;
+}
+
+/* cov: 0 exponential, 1 Gaussian.  modes: k1, k2, k3, a, b as 5 arrays of n_modes. */
+int og_kfield_modes(uint64_t seed, int n_modes, int cov, double lx, double ly, double lz,
+                    double* modes) {
+    if (n_modes <= 0 || !(lx > 0 && ly > 0 && lz > 0) || (cov != 0 && cov != 1)) return -1;
+    const double PI = 3.14159265358979323846;
+    double* k1 = modes;
+    double* k2 = modes + n_modes;
+    double* k3 = modes + 2 * (size_t)n_modes;
+    double* am = modes + 3 * (size_t)n_modes;
+    double* bm = modes + 4 * (size_t)n_modes;
+    for (int m = 0; m < n_modes; ++m) {
+        og_mode_rng g = {seed, (uint32_t)m, 0u, {0u, 0u, 0u, 0u}, 0};
+        const double fi = 2.0 * PI * og_u01(&g);
+        const double theta = acos(1.0 - 2.0 * og_u01(&g));
+        double kk = 0.0;
+        if (cov == 0) {
+            for (int tries = 0; tries < 100000; ++tries) {
+                kk = tan(PI * 0.5 * og_u01(&g));
+                if (og_u01(&g) < kk * kk / (1.0 + kk * kk)) break;
+            }
+        } else {
+            for (int tries = 0; tries < 100000; ++tries) {
+                kk = 10.0 * og_u01(&g);
+                if (og_u01(&g) * 2.0 * exp(-1.0) < kk * kk * exp(-0.5 * kk * kk)) break;
+            }
+            kk *= sqrt(2.0);
+        }
+        k1[m] = kk * sin(fi) * sin(theta) / lx;
+        k2[m] = kk * cos(fi) * sin(theta) / ly;
+        k3[m] = kk * cos(theta) / lz;
+        double u1 = og_u01(&g), u2 = og_u01(&g);
+        am[m] = sqrt(-2.0 * log(u1)) * cos(2.0 * PI * u2);
+        u1 = og_u01(&g);
+        u2 = og_u01(&g);
+        bm[m] = sqrt(-2.0 * log(u1)) * cos(2.0 * PI * u2);
+    }
+    return 0;
+}
+
+/* lnK (want_exp = 0) or K = exp(lnK + log_kg) (want_exp = 1) at cell centres, evaluated as   */
+/* the product does: per run of SEG cells along x, sin/cos of the run's first phase, then   */
+/* the phase advanced by a rotation through k_x*dx per cell.  Fast enough for 256^3 fields   */
+/* on the host; og_lnk_eval above is the direct per-cell form.                              */
+void og_kfield_eval_runs(int nx, int ny, int nz, double dx, int n_modes, const double* modes,
+                         double sigma, double log_kg, int want_exp, double* out) {
+    enum { SEG = 16 };
+    const double* k1 = modes;
+    const double* k2 = modes + n_modes;
+    const double* k3 = modes + 2 * (size_t)n_modes;
+    const double* am = modes + 3 * (size_t)n_modes;
+    const double* bm = modes + 4 * (size_t)n_modes;
+    const double scale = sigma / sqrt((double)n_modes);
+    double* sd = (double*)malloc(2 * sizeof(double) * (size_t)n_modes);
+    double* cd = sd + n_modes;
+    for (int m = 0; m < n_modes; ++m) {
+        sd[m] = sin(k1[m] * dx);
+        cd[m] = cos(k1[m] * dx);
+    }
+    const int nseg = (nx + SEG - 1) / SEG;
+#pragma omp parallel for schedule(static)
+    for (long long task = 0; task < (long long)ny * nz * nseg; ++task) {
+        const int seg = (int)(task % nseg);
+        const long long row = task / nseg;
+        const int j = (int)(row % ny), k = (int)(row / ny);
+        const int i0 = seg * SEG;
+        const double x0 = dx * (i0 + 0.5), y = dx * (j + 0.5), z = dx * (k + 0.5);
+        double acc[SEG];
+        for (int t = 0; t < SEG; ++t) acc[t] = 0.0;
+        for (int m = 0; m < n_modes; ++m) {
+            const double ph = k1[m] * x0 + k2[m] * y + k3[m] * z;
+            double s = sin(ph), c = cos(ph);
+            const double a = am[m], b = bm[m];
+            for (int t = 0; t < SEG; ++t) {
+                acc[t] += a * s + b * c;
+                const double s2 = s * cd[m] + c * sd[m];
+                c = c * cd[m] - s * sd[m];
+                s = s2;
+            }
+        }
+        for (int t = 0; t < SEG && i0 + t < nx; ++t) {
+            const double v = scale * acc[t];
+            out[IX(i0 + t, j, k)] = want_exp ? exp(v + log_kg) : v;
+        }
+    }
+    free(sd);
+}

@@ -86,6 +86,9 @@ def lib():
         L.og_velocity.argtypes = [i, i, i, d, pbc, _dp, _dp, i, _dp, _dp, _dp]
         L.og_mass_balance.argtypes = [i, i, i, d, _dp, _dp, _dp, C.c_void_p, _dp]
         L.og_lnk_eval.argtypes = [i, i, i, d, i, _dp, _dp, _dp, _dp, _dp, d, _dp]
+        L.og_kfield_modes.argtypes = [C.c_uint64, i, i, d, d, d, _dp]
+        L.og_kfield_modes.restype = i
+        L.og_kfield_eval_runs.argtypes = [i, i, i, d, i, _dp, d, d, i, _dp]
         L.og_num_threads.restype = i
         L.og_set_num_threads.argtypes = [i]
         _lib = L
@@ -241,6 +244,29 @@ def lnk_eval(shape, modes, sigma, dx=1.0):
     k1, k2, k3, a, b = (_c(m) for m in modes)
     out = np.empty(shape)
     lib().og_lnk_eval(nx, ny, nz, dx, len(a), k1, k2, k3, a, b, float(sigma), out.ravel())
+    return out
+
+
+def kfield_modes(seed, n_modes=1000, covariance=0, lam=(1.0, 1.0, 1.0)):
+    """Randomization-method modes (5, n_modes) = k1, k2, k3, a, b from the Philox sampler.
+    covariance: 0 exponential, 1 Gaussian."""
+    out = np.empty(5 * n_modes)
+    rc = lib().og_kfield_modes(int(seed) & 0xFFFFFFFFFFFFFFFF, int(n_modes), int(covariance),
+                               float(lam[0]), float(lam[1]), float(lam[2]), out)
+    if rc != 0:
+        raise ValueError("bad K-field parameters")
+    return out.reshape(5, n_modes)
+
+
+def generate_K(shape, sigma2, lam=(1.0, 1.0, 1.0), seed=0, n_modes=1000, covariance=0,
+               K_geo=1.0, dx=1.0, log_only=False):
+    """K = K_geo exp(lnK) (or lnK) on the host, for a process that must not load the product:
+    the same modes and the same run-wise evaluation as the product's generator."""
+    nz, ny, nx = shape
+    modes = np.ascontiguousarray(kfield_modes(seed, n_modes, covariance, lam)).ravel()
+    out = np.empty(shape)
+    lib().og_kfield_eval_runs(nx, ny, nz, dx, n_modes, modes, float(np.sqrt(sigma2)),
+                              float(np.log(K_geo)), 0 if log_only else 1, out.ravel())
     return out
 
 

@@ -170,3 +170,21 @@ def test_solve_once_cli_parses_without_a_gpu():
                          text=True, timeout=120, cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
     assert out.returncode == 0, out.stderr
     assert "--precision" in out.stdout and "--graph" in out.stdout
+
+
+def test_oracle_kfield_generator_matches_the_product(mf3d, oracle_mod):
+    """The oracle's host K generator (used where the product must not be loaded: the
+    reference arm of the bench) draws bit-identical modes to the product's Philox sampler,
+    and its run-wise evaluation equals the direct per-cell sum to rounding."""
+    M, O = mf3d, oracle_mod
+    for seed in (0, 20240601, 2 ** 40 + 3):
+        for cov in (0, 1):
+            for lam in ((4.0, 4.0, 4.0), (16.0, 16.0, 4.0)):
+                assert np.array_equal(O.kfield_modes(seed, 300, cov, lam), M.kfield_modes(seed, 300, cov, lam))
+    modes = O.kfield_modes(5, 200, 0, (4.0, 4.0, 4.0))
+    shape = (12, 10, 37)  # nx = 37: a ragged last run of the 16-cell x runs
+    direct = O.lnk_eval(shape, modes, 1.5)
+    runs = O.generate_K(shape, 1.5 ** 2, (4.0, 4.0, 4.0), seed=5, n_modes=200, log_only=True)
+    assert np.abs(runs - direct).max() / np.abs(direct).max() < 1e-12
+    K = O.generate_K(shape, 1.5 ** 2, (4.0, 4.0, 4.0), seed=5, n_modes=200, K_geo=2.0)
+    assert np.allclose(K, 2.0 * np.exp(runs), rtol=1e-14, atol=0)

@@ -271,6 +271,16 @@ def test_kfield_vs_oracle(mf3d, oracle_mod):
     assert np.allclose(_np(K), np.exp(ref), rtol=1e-9)
 
 
+def test_host_kfield_equals_device_kfield(mf3d, oracle_mod):
+    """The oracle's host generator (the reference arm's K) and the product's device generator
+    give the same field at the headline statistics (sigma^2 = 4, lambda = 8, 1000 modes)."""
+    M, O = mf3d, oracle_mod
+    g = M.Grid3D(64, 48, 40, 1.0)
+    K = M.generate_K_field(g, 4.0, (8.0, 8.0, 8.0), seed=20240601, n_modes=1000)
+    Ko = O.generate_K((40, 48, 64), 4.0, (8.0, 8.0, 8.0), seed=20240601, n_modes=1000)
+    assert _rel(_np(K), Ko) < 1e-12
+
+
 @pytest.mark.parametrize("prec", [0, 1])
 def test_standalone_mg_solver_vs_oracle(mf3d, oracle_mod, prec):
     """solver = mg: V-cycles on the current head until ||r||/||r0|| < rtol
