@@ -150,6 +150,19 @@ int mf3d_head_solver_vcycle(mf3d_head_solver* s, const double* r_dev, double* z_
  * a solve; the solver state is scratch afterwards and is rebuilt by the next solve).  Fills
  * up to `cap` records and sets *count. */
 int mf3d_head_solver_profile(mf3d_head_solver* s, int reps, mf3d_kernel_timing* out, int cap, int* count);
+/* Device-time limit of one solve of this solver (default 120 s; no counterpart in the
+ * reference, whose loop has only its iteration cap).  The loop's first kernel checks
+ * %globaltimer once per iteration; past the limit the solve ends with status 3 and
+ * converged = 0, and the solver stays usable. */
+int mf3d_head_solver_set_time_budget(mf3d_head_solver* s, double seconds);
+
+/* Diagnostics, no counterpart in the reference: runs the bounded mbarrier wait of the staged
+ * smoother (which = 0) or of the tensor-core convolution (which = 1) for `tries` polls on a
+ * barrier that nothing completes (arrive = 0) or that one arrival completes (arrive = 1), and
+ * reports in *gave_up_host whether the wait gave up.  No copy is in flight, so the failure
+ * path leaves the context usable. */
+int mf3d_diag_bounded_wait(int which, int arrive, int tries, int* gave_up_host);
+
 /* Kernels launched by the last mf3d_head_solver_set_K (diagnostics). */
 int mf3d_head_solver_setup_launches(const mf3d_head_solver* s);
 
@@ -165,6 +178,18 @@ int mf3d_velocity_from_head(const mf3d_grid* grid, const mf3d_bc* bc, const doub
 int mf3d_velocity_mass_balance(const mf3d_grid* grid, const mf3d_bc* bc, const double* h_dev,
                                const double* K_dev, double* U_dev, double* V_dev, double* W_dev,
                                double* out_host, void* stream);
+
+/* compute_velocity_diagnostics (src/physics/flow/velocity_diagnostics.cu:22-179): from a face
+ * velocity field (layout MF3D_VEL_*; the reference takes the padded one) the cell-centred
+ * divergence of every cell, and at the interior cells the magnitude of the curl of the
+ * face-averaged cell velocity (centred differences) and the helicity u . curl u, zero at the
+ * boundary cells and everywhere when a dimension is below 3.  div / omag / hel (device, n
+ * cells each) may be NULL to skip storing that field.  stats_host (9 doubles, may be NULL):
+ * min, max and mean of div, |omega| and helicity over all cells, as print_velocity_diagnostics
+ * reports them (velocity_diagnostics.cu:181-203). */
+int mf3d_velocity_diagnostics(const mf3d_grid* grid, int layout, const double* U_dev, const double* V_dev,
+                              const double* W_dev, double* div_dev, double* omag_dev, double* hel_dev,
+                              double* stats_host, void* stream);
 
 /* No counterpart in the reference.  Same results as mf3d_velocity_mass_balance, but its
  * reduction scratch is a static device array (64 B + 16 B per block, 262,208 B in all), so it

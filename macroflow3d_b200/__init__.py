@@ -183,6 +183,10 @@ class HeadSolver:
         return [(arr[i].name.decode(), float(arr[i].ms), float(arr[i].bytes), int(arr[i].launches_per_iter))
                 for i in range(cnt.value)]
 
+    def set_time_budget(self, seconds: float) -> None:
+        """Device-time limit of one solve (default 120 s): past it the loop ends with status 3."""
+        check(lib().mf3d_head_solver_set_time_budget(self._h, float(seconds)))
+
     def vcycle(self, r, z) -> None:
         """MultigridPreconditioner::apply (src/numerics/solvers/mg_preconditioner.cu:16-44)."""
         n = self.grid.num_cells()
@@ -492,6 +496,33 @@ def velocity_mass_balance_noalloc(U, V, W, h, K, grid: Grid3D,
         C.byref(grid.c()), C.byref(_bc(bc)), _f64(h, n, "h"), _f64(K, n, "K"),
         _f64(U, su, "U"), _f64(V, sv, "V"), _f64(W, sw, "W"), out, _stream()))
     return out[0], out[1], out[2]
+
+
+def velocity_diagnostics(U, V, W, grid: Grid3D, layout: int = VEL_PADDED, div=None, omag=None, hel=None,
+                         stats: bool = True):
+    """compute_velocity_diagnostics + the statistics print_velocity_diagnostics reports
+    (src/physics/flow/velocity_diagnostics.cu:22-203): the cell-centred divergence, |curl u| and
+    helicity are written into div / omag / hel when given (float64 CUDA tensors of n cells);
+    returns {"div": (min, max, mean), "vorticity_mag": (...), "helicity": (...)} or None."""
+    n = grid.num_cells()
+    su, sv, sw = velocity_sizes(grid, layout)
+    out = (C.c_double * 9)()
+    opt = lambda t, name: None if t is None else _f64(t, n, name)  # noqa: E731
+    check(lib().mf3d_velocity_diagnostics(C.byref(grid.c()), int(layout), _f64(U, su, "U"), _f64(V, sv, "V"),
+                                          _f64(W, sw, "W"), opt(div, "div"), opt(omag, "omag"), opt(hel, "hel"),
+                                          out if stats else None, _stream()))
+    if not stats:
+        return None
+    return {"div": tuple(out[0:3]), "vorticity_mag": tuple(out[3:6]), "helicity": tuple(out[6:9])}
+
+
+def diag_bounded_wait(which: int, arrive: bool, tries: int) -> bool:
+    """Runs one bounded mbarrier wait (0: the staged smoother's, 1: the convolution's) on a
+    barrier that nothing completes (arrive False) or that one arrival completes; True when the
+    wait gave up."""
+    out = C.c_int(-1)
+    check(lib().mf3d_diag_bounded_wait(int(which), 1 if arrive else 0, int(tries), C.byref(out)))
+    return out.value == 1
 
 
 def kfield_modes(seed: int, n_modes: int = 1000, covariance: int = COV_EXPONENTIAL,

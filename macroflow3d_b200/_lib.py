@@ -90,6 +90,9 @@ SIGNATURES = {
     "mf3d_velocity_from_head": ([_G, _B, _P, _P, C.c_int, _P, _P, _P, _P], C.c_int),
     "mf3d_velocity_mass_balance": ([_G, _B, _P, _P, _P, _P, _P, C.POINTER(C.c_double), _P], C.c_int),
     "mf3d_velocity_mass_balance_noalloc": ([_G, _B, _P, _P, _P, _P, _P, C.POINTER(C.c_double), _P], C.c_int),
+    "mf3d_head_solver_set_time_budget": ([_P, C.c_double], C.c_int),
+    "mf3d_diag_bounded_wait": ([C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)], C.c_int),
+    "mf3d_velocity_diagnostics": ([_G, C.c_int, _P, _P, _P, _P, _P, _P, C.POINTER(C.c_double), _P], C.c_int),
     "mf3d_apply_A": ([_G, _B, C.c_int, _P, _P, _P, _P], C.c_int),
     "mf3d_gsrb": ([_G, _B, C.c_int, _P, _P, _P, C.c_int, _P], C.c_int),
     "mf3d_residual": ([_G, _B, C.c_int, _P, _P, _P, _P, _P], C.c_int),

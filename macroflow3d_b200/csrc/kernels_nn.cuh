@@ -84,10 +84,10 @@ __device__ __forceinline__ void nn_mbar_init(uint64_t* bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sm_u32(bar)), "r"(count) : "memory");
 }
 // bounded wait on an mbarrier phase; false when it gave up.  Each try suspends the thread for
-// up to 2 us unless the phase completes first (fewer spinning instructions); at most 2^20 tries.
-__device__ __forceinline__ bool nn_mbar_wait(uint64_t* bar, unsigned parity) {
+// up to 2 us unless the phase completes first (fewer spinning instructions); at most `tries`.
+__device__ __forceinline__ bool nn_mbar_wait(uint64_t* bar, unsigned parity, int tries = 1 << 20) {
     const uint32_t a = sm_u32(bar);
-    for (int it = 0; it < (1 << 20); ++it) {
+    for (int it = 0; it < tries; ++it) {
         uint32_t ok;
         asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
                      : "=r"(ok)

@@ -151,6 +151,8 @@ __device__ __forceinline__ void residual_body(const LevelOp<TC>& L, const double
                 stop = 1;
             }
             if (it >= st->max_iter) stop = 1;
+            // a stop that the first block decided in this launch (body cap or time budget) stands
+            if (*reinterpret_cast<volatile int*>(&st->stop)) stop = 1;
             st->stop = stop;
             if (use_cond) cudaGraphSetConditional(cond, stop ? 0u : 1u);
         } else {
@@ -445,6 +447,9 @@ __device__ __forceinline__ void xr_update_body(size_t n, double* __restrict__ x,
             }
         }
         if (it >= s.max_iter) stop = 1;
+        // a stop that block 0 decided in this launch (body cap or time budget) stands: its store
+        // precedes its arrival at the grid sum, which precedes this block's
+        if (*reinterpret_cast<volatile int*>(&st->stop)) stop = 1;
         st->stop = stop;
         if (use_cond) cudaGraphSetConditional(cond, stop ? 0u : 1u);
     }

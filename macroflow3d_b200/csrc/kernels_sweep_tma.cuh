@@ -94,10 +94,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
                  : "memory");
 }
 
-// Bounded wait on an mbarrier phase; returns false if it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+// Bounded wait on an mbarrier phase; returns false if it gave up after `tries` polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int tries = 1 << 22) {
     const uint32_t a = smem_u32(bar);
-    for (int it = 0; it < (1 << 22); ++it) {
+    for (int it = 0; it < tries; ++it) {
         uint32_t ok;
         asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
                      : "=r"(ok)

@@ -25,9 +25,11 @@
 #include "../../include/mf3d.h"
 #include "kernels_kfield.cuh"
 #include "kernels_mg.cuh"
+#include "kernels_nn.cuh"
 #include "kernels_pcg.cuh"
 #include "kernels_resid.cuh"
 #include "kernels_setup.cuh"
+#include "kernels_sweep_pair.cuh"
 #include "kernels_sweep_tma.cuh"
 #include "kernels_tail.cuh"
 #include "kernels_velocity.cuh"
@@ -39,7 +41,8 @@ static thread_local std::string g_err;
 // Shared memory of the one-CTA coarse tail (padded x and b of its levels), at most.
 static constexpr size_t kTailSmemMax = 200 * 1024;
 
-// Device-time limit of one solve: the PCG loop stops with status 3 after this long.
+// Device-time limit of one solve by default: the PCG loop stops with status 3 after this long
+// (mf3d_head_solver_set_time_budget changes it per solver).
 static constexpr unsigned long long kSolveBudgetNs = 120ull * 1000000000ull;
 
 struct Error : std::runtime_error {
@@ -158,6 +161,47 @@ struct Geom {
     size_t n;
     double dx;
 };
+
+// Work items of the x-pair sweep: (tile, z chunk) pairs, tiles fastest, about
+// sp_items_per_cta() items per resident CTA; the grid is at most the resident CTA count and its
+// CTAs walk the items in turn.  MF3D_SWEEP_ITEMS overrides the items per CTA (tuning).
+static int sp_items_per_cta() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("MF3D_SWEEP_ITEMS");
+        v = e ? std::max(1, std::atoi(e)) : 2;
+    }
+    return v;
+}
+static dim3 pair_grid(const Geom& g, long long resident, int* zchunk) {
+    const long long tiles = (long long)((g.nx + SP_TX - 1) / SP_TX) * ((g.ny + SP_TY - 1) / SP_TY);
+    const long long want = resident * sp_items_per_cta();
+    const long long nchunk = std::max<long long>(1, std::min<long long>(g.nz, want / std::max(1LL, tiles)));
+    const int zc = (int)((g.nz + nchunk - 1) / nchunk);
+    const long long items = tiles * ((g.nz + zc - 1) / zc);
+    *zchunk = zc;
+    return dim3((unsigned)std::max(1LL, std::min(items, resident)));
+}
+
+template <class T, class TC>
+static void launch_pair_sweep(cudaStream_t s, dim3 grid, int mode, const SpArgs<T, TC>& a) {
+    const size_t smem = sp_smem_bytes<T, TC>();
+    switch (mode) {
+    case 0: sweep_pair_kernel<T, TC, 0><<<grid, SP_NT, smem, s>>>(a); break;
+    case M_ZERO: sweep_pair_kernel<T, TC, M_ZERO><<<grid, SP_NT, smem, s>>>(a); break;
+    case M_PROLONG: sweep_pair_kernel<T, TC, M_PROLONG><<<grid, SP_NT, smem, s>>>(a); break;
+    case M_ZERO | M_PROLONG: sweep_pair_kernel<T, TC, M_ZERO | M_PROLONG><<<grid, SP_NT, smem, s>>>(a); break;
+    case M_DOT: sweep_pair_kernel<T, TC, M_DOT><<<grid, SP_NT, smem, s>>>(a); break;
+    case M_ZERO | M_DOT: sweep_pair_kernel<T, TC, M_ZERO | M_DOT><<<grid, SP_NT, smem, s>>>(a); break;
+    case M_PROLONG | M_DOT: sweep_pair_kernel<T, TC, M_PROLONG | M_DOT><<<grid, SP_NT, smem, s>>>(a); break;
+    case M_ZERO | M_PROLONG | M_DOT:
+        sweep_pair_kernel<T, TC, M_ZERO | M_PROLONG | M_DOT><<<grid, SP_NT, smem, s>>>(a);
+        break;
+    default: throw Error(MF3D_E_INVALID, "unsupported x-pair sweep mode");
+    }
+    MF3D_LAUNCH_CK();
+}
+
 
 // Levels by halving every axis (MGHierarchy, src/multigrid/mg_types.hpp:86-99): at most
 // `max_levels`, stop when a coarse axis would be < 2.  An axis of odd length is never
@@ -404,6 +448,22 @@ template <class T, class TC> class VCycle : public VCycleBase {
             }
         }
         if (n_tma_) set_tma_smem();
+        // levels the x-pair sweep serves (the FP64 V-cycle; single solves, every mode but the
+        // fused residual): nx even, periodic axes a whole number of tiles.  The FP32 V-cycle keeps
+        // the TMA quad sweep, measured faster in FP32 (0.152 against 0.203 ms for a plain sweep
+        // at 256^3), where it fits two CTAs per SM
+        pair_.assign(Lt, 0);
+        if constexpr (sizeof(T) == 8 && sizeof(TC) == 8) {
+            for (int l = 0; l < Lt; ++l) {
+                const Geom& g = G[l];
+                if (g.nx % 2) continue;
+                if (bc.type[0] == MF3D_BC_PERIODIC && g.nx % SP_TX) continue;
+                if (bc.type[2] == MF3D_BC_PERIODIC && g.ny % SP_TY) continue;
+                pair_[l] = 1;
+                ++n_pair_;
+            }
+            if (n_pair_) set_pair_smem();
+        }
         // coarse tail: FP64 weights per cell, x (ghost-padded) and b in shared memory
         if (Lt < nl) {
             tail_.nlev = nl - Lt;
@@ -499,7 +559,7 @@ template <class T, class TC> class VCycle : public VCycleBase {
                 rec_sw_ = sw;
                 // staged levels: the last pre-sweep, then the residual and its restriction in a
                 // kernel of their own (batched solves keep the fused form they record)
-                const bool split = (mode & M_RESID) && tma_[l] && split_resid_ && !rec_;
+                const bool split = (mode & M_RESID) && (tma_[l] || pair_[l]) && split_resid_ && !rec_;
                 sweep(s, l, c, out, nullptr, split ? nullptr : bc_next, split ? (mode & ~M_RESID) : mode, nullptr);
                 if (split) resid_restrict(s, l, out, bc_next);
                 c = out;
@@ -551,7 +611,7 @@ template <class T, class TC> class VCycle : public VCycleBase {
             T* bc1 = (T*)bl_[1]->p;
             const T* e1 = (Lt_ == 1) ? (const T*)tail_out_->p : (const T*)xa_[1]->p;
             const int pre_extra = std::max(0, pre_ - 2), post_extra = std::max(0, post_ - 2);
-            const char* tag = tma_[0] ? "tma" : "ldg";
+            const char* tag = pair_[0] ? "pair" : (tma_[0] ? "tma" : "ldg");
             char nm[40];
             if (pre_ >= 1) {
                 std::snprintf(nm, sizeof(nm), "sweep_l0_zero_in_%s", tag);
@@ -559,7 +619,7 @@ template <class T, class TC> class VCycle : public VCycleBase {
                     sweep(tm.s, 0, nullptr, xa, nullptr, bc1, pre_ == 1 ? (M_ZERO | M_RESID) : M_ZERO, nullptr);
                 }), et * n + coef + et * n + (pre_ == 1 ? et * nc : 0.0), 1));
             }
-            if (pre_ >= 2 && tma_[0] && split_resid_) {
+            if (pre_ >= 2 && (tma_[0] || pair_[0]) && split_resid_) {
                 std::snprintf(nm, sizeof(nm), "sweep_l0_2nd_pre_%s", tag);
                 out.push_back(timing(nm, tm.mean_ms(reps, [&] {
                     sweep(tm.s, 0, xa, xb, nullptr, nullptr, 0, nullptr);
@@ -591,7 +651,7 @@ template <class T, class TC> class VCycle : public VCycleBase {
                 }), et * n + et * n + coef + et * n + 8.0 * n + (post_ == 1 ? et * nc : 0.0), 1));
             }
             for (int l = 1; l < Lt_; ++l) {
-                std::snprintf(nm, sizeof(nm), "sweep_l%d_plain_%s", l, tma_[l] ? "tma" : "ldg");
+                std::snprintf(nm, sizeof(nm), "sweep_l%d_plain_%s", l, pair_[l] ? "pair" : (tma_[l] ? "tma" : "ldg"));
                 T* a = (T*)xa_[l]->p;
                 T* b = (T*)xb_[l]->p;
                 const double nn = (double)G_[l].n;
@@ -697,6 +757,12 @@ template <class T, class TC> class VCycle : public VCycleBase {
             rec_->push_back(r);
             return;
         }
+        if constexpr (sizeof(T) == sizeof(TC)) {
+            if (pair_[l] && !(mode & M_RESID)) {
+                pair_sweep(s, l, x_in, x_out, e, mode, dot_out);
+                return;
+            }
+        }
         const int tx = tma ? TmaSweepCfg<T, TC, 0>::TX : SW_TX, ty = tma ? tma_ty() : SW_TY;
         const int gx = (g.nx + tx - 1) / tx, gy = (g.ny + ty - 1) / ty;
         if (tma) {
@@ -750,6 +816,54 @@ template <class T, class TC> class VCycle : public VCycleBase {
     }
 
     static int tma_ty() { return TmaSweepCfg<T, TC, 0>::TY; }
+
+    // ---- the x-pair sweep (kernels_sweep_pair.cuh) ----
+    template <int MODE> void set_pair_one() {
+        if constexpr (sizeof(T) == sizeof(TC)) {
+            const size_t smem = sp_smem_bytes<T, TC>();
+            MF3D_CK(cudaFuncSetAttribute(sweep_pair_kernel<T, TC, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+            MF3D_CK(cudaFuncSetAttribute(sweep_pair_kernel<T, TC, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         (int)cudaSharedmemCarveoutMaxShared));
+            int n = 0;
+            MF3D_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_pair_kernel<T, TC, MODE>, SP_NT, smem));
+            if (n < 1) throw Error(MF3D_E_CUDA, "x-pair sweep does not fit on an SM");
+            pocc_[MODE & 15] = n;
+        }
+    }
+    void set_pair_smem() {
+        set_pair_one<0>();
+        set_pair_one<M_ZERO>();
+        set_pair_one<M_PROLONG>();
+        set_pair_one<M_ZERO | M_PROLONG>();
+        set_pair_one<M_DOT>();
+        set_pair_one<M_ZERO | M_DOT>();
+        set_pair_one<M_PROLONG | M_DOT>();
+        set_pair_one<M_ZERO | M_PROLONG | M_DOT>();
+    }
+    void pair_sweep(cudaStream_t s, int l, const T* x_in, T* x_out, const T* e, int mode, double* dot_out) {
+        if constexpr (sizeof(T) == sizeof(TC)) {
+            const Geom& g = G_[l];
+            SpArgs<T, TC> a{};
+            a.L = ops_[l];
+            a.x_in = x_in;
+            a.b = l == 0 ? b0_ : (const T*)bl_[l]->p;
+            a.x_out = x_out;
+            a.e_c = e;
+            if (l + 1 < (int)G_.size()) {
+                a.ncx = G_[l + 1].nx;
+                a.ncy = G_[l + 1].ny;
+            }
+            a.r64 = r64_;
+            a.dot_partials = scr_.partials;
+            a.dot_ticket = scr_.tickets + 0;
+            a.dot_out = dot_out;
+            const long long resident = (long long)std::max(1, pocc_[mode & 15]) * num_sms();
+            const dim3 grid = pair_grid(g, resident, &a.zchunk);
+            if ((mode & M_DOT) && grid.x > scr_.partial_cap) throw Error(MF3D_E_INVALID, "reduction scratch too small");
+            launch_pair_sweep<T, TC>(s, grid, mode, a);
+        }
+    }
 
     template <int MODE>
     static void launch_tma(cudaStream_t s, dim3 grid, const TmaMaps& m, const TmaSweepArgs<T, TC>& a) {
@@ -844,6 +958,9 @@ template <class T, class TC> class VCycle : public VCycleBase {
     // the fused sweep (cp.async moves at least 4 bytes).
     static constexpr bool split_resid_ = sizeof(TC) >= 4;
     int occ_[16] = {}; // resident staged-sweep CTAs per SM, by mode
+    std::vector<int> pair_; // levels served by the x-pair sweep
+    int n_pair_ = 0;
+    int pocc_[16] = {}; // resident x-pair-sweep CTAs per SM, by mode
     std::unique_ptr<DevMem> tail_out_, tail_w_;
     Tail2Args tail_{};
     size_t tail_smem_ = 0;
@@ -1030,6 +1147,7 @@ class HeadSolver {
     }
 
     int setup_launches() const { return setup_launches_; }
+    void set_budget_ns(unsigned long long ns) { budget_ns_ = ns; }
 
     void vcycle(const double* r, double* z) {
         if (!have_K_) throw Error(MF3D_E_STATE, "set_K must be called before vcycle");
@@ -1072,7 +1190,7 @@ class HeadSolver {
         const bool mg = cfg_.solver == MF3D_SOLVER_MG, cg = cfg_.solver == MF3D_SOLVER_CG;
         pcg_init_kernel<<<1, 1, 0, s>>>(state_.as<PcgState>(), mg ? cfg_.mg_max_cycles : cfg_.cg_max_iter,
                                         mg ? 1 : cfg_.cg_check_every, (flexible_ && !cg) ? 1 : 0,
-                                        mg ? cfg_.rtol : cfg_.cg_rtol, kSolveBudgetNs, cfg_.solver);
+                                        mg ? cfg_.rtol : cfg_.cg_rtol, budget_ns_, cfg_.solver);
         MF3D_LAUNCH_CK();
         launch_residual(s, 0);
         if (cfg_.use_graph) {
@@ -1151,6 +1269,7 @@ class HeadSolver {
     cudaStream_t stream() const { return stream_; }
 
   private:
+    unsigned long long budget_ns_ = kSolveBudgetNs;
     // p = z + beta p fused with Ap = A p and <p, Ap> (z = r for plain CG)
     void launch_pmatvec(cudaStream_t s) {
         PcgState* st = state_.as<PcgState>();
@@ -1436,6 +1555,41 @@ int mf3d_head_solver_setup_launches(const mf3d_head_solver* s) {
     return s ? s->impl->setup_launches() : MF3D_E_INVALID;
 }
 
+int mf3d_head_solver_set_time_budget(mf3d_head_solver* s, double seconds) {
+    return guard([&] {
+        need(s, "solver");
+        if (!(seconds > 0.0) || seconds > 1e6) throw Error(MF3D_E_INVALID, "time budget must be in (0, 1e6] seconds");
+        s->impl->set_budget_ns((unsigned long long)(seconds * 1e9));
+    });
+}
+
+// Bounded-wait self-test: an mbarrier whose phase nothing completes (arrive = 0) or that one
+// arrival completes (arrive = 1), waited on by one thread with `tries` polls of the smoother's
+// wait (which = 0) or the convolution's (which = 1).  No copy is in flight: giving up leaves
+// nothing behind.
+__global__ void bounded_wait_kernel(int which, int arrive, int tries, int* out) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (arrive) mbar_arrive(&bar);
+    const bool ok = which == 0 ? mbar_wait(&bar, 0u, tries) : nn::nn_mbar_wait(&bar, 0u, tries);
+    out[0] = ok ? 0 : 1;
+}
+
+int mf3d_diag_bounded_wait(int which, int arrive, int tries, int* gave_up_host) {
+    return guard([&] {
+        need(gave_up_host, "gave_up_host");
+        if ((which != 0 && which != 1) || tries < 1 || tries > (1 << 22))
+            throw Error(MF3D_E_INVALID, "which must be 0 or 1, tries in [1, 2^22]");
+        DevMem out(sizeof(int));
+        MF3D_CK(cudaMemset(out.p, 0xff, sizeof(int)));
+        bounded_wait_kernel<<<1, 32>>>(which, arrive ? 1 : 0, tries, out.as<int>());
+        MF3D_LAUNCH_CK();
+        MF3D_CK(cudaMemcpy(gave_up_host, out.p, sizeof(int), cudaMemcpyDeviceToHost));
+    });
+}
+
 int mf3d_head_solver_profile(mf3d_head_solver* s, int reps, mf3d_kernel_timing* out, int cap, int* count) {
     return guard([&] {
         need(s, "solver");
@@ -1510,6 +1664,30 @@ int mf3d_velocity_mass_balance(const mf3d_grid* g, const mf3d_bc* bc, const doub
     return guard([&] {
         need(out_host, "out_host");
         run_velocity(g, bc, h, K, MF3D_VEL_COMPACT, U, V, W, out_host, (cudaStream_t)stream);
+    });
+}
+
+int mf3d_velocity_diagnostics(const mf3d_grid* g, int layout, const double* U, const double* V, const double* W,
+                              double* div, double* omag, double* hel, double* stats_host, void* stream) {
+    return guard([&] {
+        check_grid(g);
+        need(U, "U");
+        need(V, "V");
+        need(W, "W");
+        if (layout != MF3D_VEL_COMPACT && layout != MF3D_VEL_PADDED) throw Error(MF3D_E_INVALID, "unknown layout");
+        cudaStream_t s = (cudaStream_t)stream;
+        const ColLaunch cl = col_launch(g->nx, g->ny, g->nz);
+        // temporary reduction scratch, as the reference's compute_field_stats allocates its own
+        DevMem scr(stats_host ? (9 * (size_t)cl.nblocks + 16) * sizeof(double) : 0);
+        double* partials = stats_host ? scr.as<double>() : nullptr;
+        double* stats_dev = stats_host ? partials + 9 * (size_t)cl.nblocks : nullptr;
+        unsigned* ticket = stats_host ? reinterpret_cast<unsigned*>(stats_dev + 9) : nullptr;
+        if (stats_host) MF3D_CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned), s));
+        velocity_diag_kernel<<<cl.grid, cl.block, 0, s>>>(g->nx, g->ny, g->nz, 1.0 / g->dx, layout, U, V, W, div,
+                                                          omag, hel, partials, ticket, stats_dev, cl.zchunk);
+        MF3D_LAUNCH_CK();
+        if (stats_host) MF3D_CK(cudaMemcpyAsync(stats_host, stats_dev, 9 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        MF3D_CK(cudaStreamSynchronize(s));
     });
 }
 
@@ -1672,6 +1850,30 @@ int mf3d_gsrb(const mf3d_grid* g, const mf3d_bc* bc, int pin, const double* K, c
         OneLevel L(g, bc, pin, K, s);
         if (iters == 0) return;
         DevMem tmp(L.G.n * sizeof(double));
+        double* pbufs[2] = {x, tmp.as<double>()};
+        // the x-pair sweep where it applies (nx even, periodic axes whole tiles), as in the V-cycle
+        if (g->nx % 2 == 0 && (bc->type[0] != MF3D_BC_PERIODIC || g->nx % SP_TX == 0) &&
+            (bc->type[2] != MF3D_BC_PERIODIC || g->ny % SP_TY == 0)) {
+            const size_t smem = sp_smem_bytes<double, double>();
+            MF3D_CK(cudaFuncSetAttribute(sweep_pair_kernel<double, double, 0>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            int occ = 0;
+            MF3D_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sweep_pair_kernel<double, double, 0>, SP_NT, smem));
+            SpArgs<double, double> a{};
+            a.L = L.op;
+            a.b = b;
+            const dim3 grid = pair_grid(L.G, (long long)std::max(1, occ) * num_sms(), &a.zchunk);
+            int cur = 0;
+            for (int it = 0; it < iters; ++it) {
+                a.x_in = pbufs[cur];
+                a.x_out = pbufs[cur ^ 1];
+                launch_pair_sweep<double, double>(s, grid, 0, a);
+                cur ^= 1;
+            }
+            if (cur != 0) MF3D_CK(cudaMemcpyAsync(x, pbufs[cur], L.G.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            MF3D_CK(cudaStreamSynchronize(s));
+            return;
+        }
         const int gx = (g->nx + SW_TX - 1) / SW_TX, gy = (g->ny + SW_TY - 1) / SW_TY;
         const int zc = std::max(2, std::min(64, ((g->nz + 1) & ~1)));
         dim3 grid(gx, gy, (g->nz + zc - 1) / zc);

@@ -897,3 +897,80 @@ void og_kfield_eval_runs(int nx, int ny, int nz, double dx, int n_modes, const d
     }
     free(sd);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Velocity diagnostics at cell centres                                      */
+/* src/physics/flow/velocity_diagnostics.cu:48-141 (kernel) and :147-179      */
+/* (host): divergence at every cell; |curl u| and helicity u.curl u from      */
+/* centred differences of face-averaged cell velocities at interior cells     */
+/* (1 <= i <= nx-2, ...), zero elsewhere and everywhere when a dimension is   */
+/* below 3.  layout 1 is the reference's padded layout (padded_layout.cuh:30),*/
+/* layout 0 the compact MAC arrays.  stats (9 doubles, may be NULL): min, max,*/
+/* mean of div, |omega|, helicity over all cells (the mean as the reference's */
+/* compute_field_stats gives it, stochastic.cu:369-415: sum / n).             */
+/* ------------------------------------------------------------------------ */
+static inline size_t og_ui(int lay, int i, int j, int k, int nx, int ny) {
+    return lay ? (size_t)k * (ny + 1) * (nx + 1) + (size_t)j * (nx + 1) + (size_t)i
+               : (size_t)i + (size_t)j * (nx + 1) + (size_t)k * (nx + 1) * ny;
+}
+static inline size_t og_vi(int lay, int i, int j, int k, int nx, int ny) {
+    return lay ? (size_t)k * (ny + 1) * (nx + 1) + (size_t)j * (nx + 1) + (size_t)i
+               : (size_t)i + (size_t)j * nx + (size_t)k * nx * (ny + 1);
+}
+static inline size_t og_wi(int lay, int i, int j, int k, int nx, int ny) {
+    return lay ? (size_t)k * (ny + 1) * (nx + 1) + (size_t)j * (nx + 1) + (size_t)i
+               : (size_t)i + (size_t)j * nx + (size_t)k * nx * ny;
+}
+
+void og_velocity_diagnostics(int nx, int ny, int nz, double dx, int lay, const double* U,
+                             const double* V, const double* W, double* div, double* omag,
+                             double* hel, double* stats) {
+    const double inv = 1.0 / dx, inv2 = 0.5 * inv;
+    const int curl = nx >= 3 && ny >= 3 && nz >= 3;
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                const size_t c = IX(i, j, k);
+                const double Ui = U[og_ui(lay, i, j, k, nx, ny)], Uip = U[og_ui(lay, i + 1, j, k, nx, ny)];
+                const double Vj = V[og_vi(lay, i, j, k, nx, ny)], Vjp = V[og_vi(lay, i, j + 1, k, nx, ny)];
+                const double Wk = W[og_wi(lay, i, j, k, nx, ny)], Wkp = W[og_wi(lay, i, j, k + 1, nx, ny)];
+                div[c] = (Uip - Ui) * inv + (Vjp - Vj) * inv + (Wkp - Wk) * inv;
+                if (!curl || i < 1 || i > nx - 2 || j < 1 || j > ny - 2 || k < 1 || k > nz - 2) {
+                    omag[c] = 0.0;
+                    hel[c] = 0.0;
+                    continue;
+                }
+#define UC(a, b, d) (0.5 * (U[og_ui(lay, a, b, d, nx, ny)] + U[og_ui(lay, (a) + 1, b, d, nx, ny)]))
+#define VC(a, b, d) (0.5 * (V[og_vi(lay, a, b, d, nx, ny)] + V[og_vi(lay, a, (b) + 1, d, nx, ny)]))
+#define WC(a, b, d) (0.5 * (W[og_wi(lay, a, b, d, nx, ny)] + W[og_wi(lay, a, b, (d) + 1, nx, ny)]))
+                const double uc = 0.5 * (Ui + Uip), vc = 0.5 * (Vj + Vjp), wc = 0.5 * (Wk + Wkp);
+                const double dwdy = (WC(i, j + 1, k) - WC(i, j - 1, k)) * inv2;
+                const double dvdz = (VC(i, j, k + 1) - VC(i, j, k - 1)) * inv2;
+                const double dudz = (UC(i, j, k + 1) - UC(i, j, k - 1)) * inv2;
+                const double dwdx = (WC(i + 1, j, k) - WC(i - 1, j, k)) * inv2;
+                const double dvdx = (VC(i + 1, j, k) - VC(i - 1, j, k)) * inv2;
+                const double dudy = (UC(i, j + 1, k) - UC(i, j - 1, k)) * inv2;
+#undef UC
+#undef VC
+#undef WC
+                const double ox = dwdy - dvdz, oy = dudz - dwdx, oz = dvdx - dudy;
+                omag[c] = sqrt(ox * ox + oy * oy + oz * oz);
+                hel[c] = uc * ox + vc * oy + wc * oz;
+            }
+    if (stats) {
+        const double* f[3] = {div, omag, hel};
+        const size_t n = (size_t)nx * ny * nz;
+        for (int q = 0; q < 3; ++q) {
+            double mn = f[q][0], mx = f[q][0], s = 0.0;
+            for (size_t c = 0; c < n; ++c) {
+                mn = f[q][c] < mn ? f[q][c] : mn;
+                mx = f[q][c] > mx ? f[q][c] : mx;
+                s += f[q][c];
+            }
+            stats[3 * q] = mn;
+            stats[3 * q + 1] = mx;
+            stats[3 * q + 2] = s / (double)n;
+        }
+    }
+}

@@ -86,6 +86,7 @@ def lib():
         L.og_velocity.argtypes = [i, i, i, d, pbc, _dp, _dp, i, _dp, _dp, _dp]
         L.og_mass_balance.argtypes = [i, i, i, d, _dp, _dp, _dp, C.c_void_p, _dp]
         L.og_lnk_eval.argtypes = [i, i, i, d, i, _dp, _dp, _dp, _dp, _dp, d, _dp]
+        L.og_velocity_diagnostics.argtypes = [i, i, i, d, i, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
         L.og_kfield_modes.argtypes = [C.c_uint64, i, i, d, d, d, _dp]
         L.og_kfield_modes.restype = i
         L.og_kfield_eval_runs.argtypes = [i, i, i, d, i, _dp, d, d, i, _dp]
@@ -236,6 +237,18 @@ def mass_balance(U, V, W, dx=1.0):
     lib().og_mass_balance(nx, ny, nz, dx, U.ravel(), V.ravel(), W.ravel(),
                           div.ctypes.data_as(C.c_void_p), out)
     return div, out[0], out[1], out[2]
+
+
+def velocity_diagnostics(U, V, W, shape, dx=1.0, layout=1):
+    """Cell-centred divergence, |curl u| and helicity (nz, ny, nx) each, and the statistics
+    [min, max, mean] x (div, |omega|, helicity)."""
+    U, V, W = _c(U), _c(V), _c(W)
+    nz, ny, nx = shape
+    div, om, he = np.empty(shape), np.empty(shape), np.empty(shape)
+    st = np.empty(9)
+    lib().og_velocity_diagnostics(nx, ny, nz, dx, layout, U.ravel(), V.ravel(), W.ravel(), div.ravel(),
+                                  om.ravel(), he.ravel(), st)
+    return div, om, he, st
 
 
 def lnk_eval(shape, modes, sigma, dx=1.0):

@@ -207,3 +207,33 @@ def test_nonfinite_realisation_does_not_stop_the_others(mf3d):
         assert rb.converged and abs(rb.num_iterations - rr.num_iterations) <= 1
         assert _rel(hb, hr) < HEAD_TOL
     b.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_batch_vs_oracle(mf3d, oracle_mod, prec):
+    """Three uneven realisations (non-cubic coarse grids) solved as one batch, each against the
+    FP64 oracle at the same tolerance (the realisation loop the batch replaces:
+    src/runtime/ensemble/EnsembleRunner.cu:259-317).  FP64: the reference algorithm, same
+    iteration count, heads equal to rounding (measured 1e-14).  FP32 V-cycle: iterations within
+    one, heads within the tolerance's reach (measured 1.2e-9)."""
+    M, O = mf3d, oracle_mod
+    shapes = [(64, 96, 64), (96, 64, 128), (128, 64, 96)]
+    grids = [M.Grid3D(*s) for s in shapes]
+    Ks = _fields(M, grids, seed=500)
+    cfg = _cfg(M, getattr(M, "PREC_" + prec.upper()))
+    b, out, _ = _batch(M, grids, M.BCSpec.darcy_x(), cfg, Ks)
+    b.close()
+    bc = O.baseline_bc()
+    for (h, res), K, g in zip(out, Ks, grids):
+        Kn = K.cpu().numpy()
+        rhs = O.build_rhs(Kn, bc)
+        r0 = np.linalg.norm(rhs - O.apply_A(Kn, O.init_guess(Kn.shape, bc), bc))
+        ho, ro = O.solve_head_pcg(Kn, bc, 8, rtol=1e-10 * np.linalg.norm(rhs) / r0, check_every=1, max_iter=200)
+        assert res.converged and ro.converged
+        assert res.true_rel_residual <= 1e-10
+        if prec == "fp64":
+            assert res.num_iterations == ro.iterations
+            assert _rel(h, ho) < 1e-12
+        else:
+            assert abs(res.num_iterations - ro.iterations) <= 1
+            assert _rel(h, ho) < 5e-9

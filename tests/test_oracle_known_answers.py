@@ -153,3 +153,38 @@ def test_mg_solver_converges(oracle_mod):
     K = np.exp(np.random.default_rng(11).normal(size=(16, 16, 16)))
     h, res = O.solve_head_mg(K, _darcy_bc(O), mg_levels=3, max_cycles=50, rtol=1e-9)
     assert res.converged and res.final_residual / res.initial_residual < 1e-9
+
+
+def test_velocity_diagnostics_known_answers(oracle_mod):
+    """Solid-body rotation about z plus a uniform axial velocity c: u = -y, v = x, w = c, so
+    div u = 0, curl u = (0, 0, 2) at every interior cell and helicity = 2c; boundary cells and
+    grids with a dimension below 3 report zero curl (velocity_diagnostics.cu:82-87)."""
+    O = oracle_mod
+    nz, ny, nx, dx, c = 5, 6, 7, 0.5, 0.75
+    for layout in (0, 1):
+        if layout:
+            shp = (nz + 1, ny + 1, nx + 1)
+            U, V, W = np.zeros(shp), np.zeros(shp), np.zeros(shp)
+            kk, jj, ii = np.meshgrid(np.arange(nz + 1), np.arange(ny + 1), np.arange(nx + 1), indexing="ij")
+            U[:] = -(jj + 0.5) * dx
+            V[:] = (ii + 0.5) * dx
+            W[:] = c
+        else:
+            kk, jj, ii = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx + 1), indexing="ij")
+            U = -(jj + 0.5) * dx
+            kk, jj, ii = np.meshgrid(np.arange(nz), np.arange(ny + 1), np.arange(nx), indexing="ij")
+            V = (ii + 0.5) * dx
+            W = np.full((nz + 1, ny, nx), c)
+        div, om, he, st = O.velocity_diagnostics(U, V, W, (nz, ny, nx), dx, layout)
+        assert np.abs(div).max() < 1e-14
+        inner = (slice(1, -1),) * 3
+        assert np.allclose(om[inner], 2.0, rtol=1e-14) and np.allclose(he[inner], 2.0 * c, rtol=1e-14)
+        mask = np.ones(om.shape, bool)
+        mask[inner] = False
+        assert not om[mask].any() and not he[mask].any()
+        ninner = (nz - 2) * (ny - 2) * (nx - 2)
+        assert np.allclose(st[3:6], [0.0, 2.0, 2.0 * ninner / om.size], rtol=1e-14)
+    # a dimension below 3: divergence only
+    U, V, W = np.ones((2, 4, 5)), np.ones((2, 5, 4)), np.ones((3, 4, 4))
+    div, om, he, st = O.velocity_diagnostics(U, V, W, (2, 4, 4), 1.0, 0)
+    assert not om.any() and not he.any() and np.abs(div).max() == 0.0
