@@ -420,8 +420,10 @@ def cpu_baseline(K_np, n, budget_s=60.0, reps=3):
             "iterations": iters}
 
 
-def roofline(prof, hbm, src):
-    """Dominant kernel by time per PCG iteration; achieved = algorithmic bytes / launch time."""
+def roofline(prof, hbm, src, precision):
+    """Dominant kernel by time per PCG iteration; achieved = algorithmic bytes / launch time.
+    traffic: the DRAM bytes of one launch of that kernel in this precision's solver, from an ncu
+    capture summarised in profiles/traffic.json (keyed by V-cycle precision, then kernel)."""
     best = None
     for name, ms, nbytes, per_iter in prof:
         if nbytes <= 0 or per_iter <= 0:
@@ -436,7 +438,7 @@ def roofline(prof, hbm, src):
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
-        traffic = json.load(open(tp)).get(name)
+        traffic = json.load(open(tp)).get(precision, {}).get(name)
     return {"kernel": name, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
             "frac": round(ach / hbm, 4), "peak_source": src, "traffic": traffic,
             "alg_bytes_per_launch": nbytes, "ms_per_launch": round(ms, 5)}
@@ -546,7 +548,7 @@ def main():
 
     if rank == 0:
         prof = out["solver"].profile(reps=10)
-        line["roofline"] = roofline(prof, hbm, src)
+        line["roofline"] = roofline(prof, hbm, src, args.precision)
         if args.profile_kernels:
             line["kernels"] = [{"name": a, "ms": round(b, 5), "GBps": round(c / (b * 1e-3) / 1e9, 1) if b > 0 else None,
                                 "per_iter": d} for a, b, c, d in prof]

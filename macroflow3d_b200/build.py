@@ -1,4 +1,4 @@
-"""Builds libmf3d.so in-tree for sm_100a (nvcc, no JIT cache), and the CPU oracle.
+"""Builds libmf3d.so in-tree for sm_100a (nvcc, no JIT cache).
 
 Usage: python -m macroflow3d_b200.build [--force]
 """
@@ -57,12 +57,6 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
     return LIB
-
-
-def build_oracle() -> str:
-    sys.path.insert(0, ROOT)
-    from oracle import oracle  # noqa: E402  (checker build only)
-    return oracle.build()
 
 
 if __name__ == "__main__":

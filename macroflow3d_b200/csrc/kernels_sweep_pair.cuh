@@ -36,6 +36,7 @@
 // correction to the pairs it staged before the barrier that publishes them.
 #pragma once
 #include <cstddef>
+#include <type_traits>
 
 #include "kernels_mg.cuh"
 #include "kernels_pcg.cuh"
@@ -107,6 +108,12 @@ template <class T> __device__ __forceinline__ void sp_stg2(T* p, T a, T b) {
     else *reinterpret_cast<float2*>(p) = make_float2(a, b);
 }
 
+// cp.async of B bytes (4, 8 or 16) to a shared address; `ok` false reads nothing and zero-fills
+template <int B> __device__ __forceinline__ void sp_cp(uint32_t dst, const char* src, bool ok) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(dst), "l"(src), "n"(B), "r"(ok ? B : 0)
+                 : "memory");
+}
+
 template <class T, class TC, int MODE>
 __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const SpArgs<T, TC> a) {
     static_assert(sizeof(T) == sizeof(TC) && sizeof(T) >= 4, "FP64 or FP32 vectors with coefficients of the same type");
@@ -116,8 +123,12 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const S
     using XS = SpXSlot<T>;
     using CS = SpCSlot<T, TC>;
     extern __shared__ __align__(16) unsigned char sp_sm[];
-    XS* xsl = reinterpret_cast<XS*>(sp_sm);
-    CS* csl = reinterpret_cast<CS*>(sp_sm + SP_NSX * sizeof(XS));
+    T* const xs0 = reinterpret_cast<T*>(sp_sm); // x slot s starts at xs0 + s * XE
+    constexpr int XE = (int)(sizeof(XS) / sizeof(T));
+    constexpr int CE = (int)(sizeof(CS) / sizeof(T));
+    T* const cs0 = reinterpret_cast<T*>(sp_sm + SP_NSX * sizeof(XS)); // coefficient slot s at cs0 + s * CE
+    constexpr int OB = 0, OCX = SP_CR * W, OCY = 2 * SP_CR * W, OCZ = 2 * SP_CR * W + SP_YR * W; // arrays in a slot
+    const uint32_t xs0_u = (uint32_t)__cvta_generic_to_shared(xs0), cs0_u = (uint32_t)__cvta_generic_to_shared(cs0);
 
     const LevelOp<TC>& L = a.L;
     const int nx = L.nx, ny = L.ny, nz = L.nz;
@@ -133,6 +144,10 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const S
     // role 0: tile pair (red + black + output); 1: ring-row pair (red); 2: ring-column cell (red)
     const int role = warp < 8 ? 0 : (warp == 8 ? 1 : 2);
     const int hi = lane >> 4, lo = lane & 15;
+    // tile warps cover rows {r, r+2}: the red offset o = (j + t) & 1 is the same for the whole warp
+    const int tyr = 4 * (warp >> 1) + (warp & 1) + 2 * hi;
+    auto nxs = [](int s) { return s + 1 == SP_NSX ? 0 : s + 1; };
+    auto ncs = [](int s) { return s + 1 == SP_NSC ? 0 : s + 1; };
     double dot_acc = 0.0;
 
     for (int item = blockIdx.x; item < total; item += gridDim.x) {
@@ -140,111 +155,12 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const S
         const int tile = item % ntiles;
         const int z0 = (item / ntiles) * a.zchunk, z1 = min(z0 + a.zchunk, nz);
         const int i0 = (tile % ntx) * SP_TX, j0 = (tile / ntx) * SP_TY;
-        // ---- this thread's pair (first cell pi, row pj; both may lie outside the grid) ----
-        int pj, pi, side = -1;
-        if (role == 0) pj = j0 + 2 * warp + hi, pi = i0 + 2 * lo;
-        else if (role == 1) pj = hi ? j0 + SP_TY : j0 - 1, pi = i0 + 2 * lo;
-        else side = hi, pj = j0 + lo, pi = hi ? i0 + SP_TX : i0 - 2;
-        // tile pairs lie inside [0, n) or beyond a partial tile's edge (never wrapped: a periodic
-        // axis is a whole number of tiles); ring pairs wrap on periodic axes
-        const int wi = role == 0 ? (pi < nx ? pi : -1) : wrap_or_out(pi, nx, L.per_x);
-        const int wj = role == 0 ? (pj < ny ? pj : -1) : wrap_or_out(pj, ny, L.per_y);
-        const bool pin_xy = wi >= 0 && wj >= 0; // both cells (nx is even)
-        const long long gxy = pin_xy ? (long long)wi + (long long)nx * wj : 0;
-        const int fx = (pj - j0 + 2) * W + (pi - i0 + 2); // x slot; cy slot too
-        const int fc = fx - W;                            // b, cx, cz slots (rows from j0-1)
-        // secondary x pair: ring-row warp the outer rows, ring-column lanes 0/1/16/17 the corners
-        int sj = 0, si = 0;
-        bool has2 = false;
-        if (role == 1) has2 = true, sj = hi ? j0 + SP_TY + 1 : j0 - 2, si = pi;
-        else if (role == 2 && (lo == 0 || lo == 1)) has2 = true, sj = lo ? j0 + SP_TY : j0 - 1, si = pi;
-        const int wi2 = wrap_or_out(si, nx, L.per_x), wj2 = wrap_or_out(sj, ny, L.per_y);
-        const bool pin2 = has2 && wi2 >= 0 && wj2 >= 0;
-        const long long gxy2 = pin2 ? (long long)wi2 + (long long)nx * wj2 : 0;
-        const int fx2 = (sj - j0 + 2) * W + (si - i0 + 2);
-        // coefficient copies beyond the primary pair's b, cx, cy, cz:
-        //   cx of a corner pair (ring-column lanes 0 / 1: rows j0-1, j0+TY, left side)
-        //   cy of the row below the ring row (ring-row lanes 0-15) or of a corner (ring-column
-        //   lanes 0 / 16: row j0-1)
-        const bool cx2 = role == 2 && side == 0 && (lo == 0 || lo == 1);
-        const bool cy2 = (role == 1 && !hi) || (role == 2 && lo == 0);
-        const int cy2j = role == 1 ? j0 - 2 : j0 - 1;
-        const int wcy2 = wrap_or_out(cy2j, ny, L.per_y);
-        // primary cx: at the -x boundary (pair -2, -1 of a non-periodic axis) the -x faces bxm
-        const bool cx_bnd = pi == -2 && !L.per_x;
-        const bool cx2_bnd = cx_bnd; // corners share the column
-        // primary cy / corner cy: on row -1 of a non-periodic axis the -y faces bym
-        const bool cy_bnd = pj == -1 && !L.per_y;
-        const bool cy2_bnd = cy2j == -1 && !L.per_y;
-
-        const int P0 = z0 - 2;               // first x plane staged
-        const int XL = z1 + 1, CL = z1;      // last x plane, last coefficient plane
-        auto xslot = [&](int p) -> XS& { return xsl[(unsigned)(p - P0) % SP_NSX]; };
-        auto cslot = [&](int p) -> CS& { return csl[(unsigned)(p - P0) % SP_NSC]; };
-
-        // one commit group: x plane p and the coefficients of plane p - 1
-        auto issue = [&](int p) {
-            if (!ZERO && p <= XL) {
-                const int kz = wrap_or_out(p, nz, L.per_z);
-                const size_t ko = nxy * (size_t)(kz < 0 ? 0 : kz);
-                XS& S = xslot(p);
-                const bool ok = pin_xy && kz >= 0;
-                pmv_cp<2 * ST>(&S.x[0][0] + fx, a.x_in + (ok ? (size_t)gxy + ko : 0), ok);
-                if (has2) {
-                    const bool ok2 = pin2 && kz >= 0;
-                    pmv_cp<2 * ST>(&S.x[0][0] + fx2, a.x_in + (ok2 ? (size_t)gxy2 + ko : 0), ok2);
-                }
-            }
-            const int q = p - 1;
-            if (q >= P0 && q <= CL) {
-                const int kz = wrap_or_out(q, nz, L.per_z);
-                const bool kin = kz >= 0;
-                const size_t ko = nxy * (size_t)(kin ? kz : 0);
-                CS& C = cslot(q);
-                const bool ok = pin_xy && kin;
-                const size_t g = ok ? (size_t)gxy + ko : 0;
-                pmv_cp<2 * ST>(&C.b[0][0] + fc, a.b + g, ok);
-                if (cx_bnd) { // -x faces of cell (0, pj): one value into the column of cell -1
-                    const bool okb = wj >= 0 && kin;
-                    pmv_cp<ST>(&C.cx[0][0] + fc + 1, L.bxm + (okb ? (size_t)wj + (size_t)ny * kz : 0), okb);
-                } else {
-                    pmv_cp<2 * ST>(&C.cx[0][0] + fc, L.cx + g, ok);
-                }
-                if (cy_bnd) { // -y faces of the pair's cells in row 0
-                    const bool okb = wi >= 0 && kin;
-                    pmv_cp<2 * ST>(&C.cy[0][0] + fx, L.bym + (okb ? (size_t)wi + (size_t)nx * kz : 0), okb);
-                } else {
-                    pmv_cp<2 * ST>(&C.cy[0][0] + fx, L.cy + g, ok);
-                }
-                if (q == -1 && !L.per_z) { // the -z faces of plane 0 stand in for plane -1's +z faces
-                    pmv_cp<2 * ST>(&C.cz[0][0] + fc, L.bzm + (pin_xy ? (size_t)gxy : 0), pin_xy);
-                } else {
-                    pmv_cp<2 * ST>(&C.cz[0][0] + fc, L.cz + g, ok);
-                }
-                if (cx2) {
-                    const int fcc = (sj - j0 + 1) * W + (si - i0 + 2);
-                    if (cx2_bnd) {
-                        const bool okb = wj2 >= 0 && kin;
-                        pmv_cp<ST>(&C.cx[0][0] + fcc + 1, L.bxm + (okb ? (size_t)wj2 + (size_t)ny * kz : 0), okb);
-                    } else {
-                        const bool ok2 = pin2 && kin;
-                        pmv_cp<2 * ST>(&C.cx[0][0] + fcc, L.cx + (ok2 ? (size_t)gxy2 + ko : 0), ok2);
-                    }
-                }
-                if (cy2) {
-                    const int fyy = (cy2j - j0 + 2) * W + (pi - i0 + 2);
-                    if (cy2_bnd) {
-                        const bool okb = wi >= 0 && kin;
-                        pmv_cp<2 * ST>(&C.cy[0][0] + fyy, L.bym + (okb ? (size_t)wi + (size_t)nx * kz : 0), okb);
-                    } else {
-                        const bool ok2 = wi >= 0 && wcy2 >= 0 && kin;
-                        pmv_cp<2 * ST>(&C.cy[0][0] + fyy,
-                                       L.cy + (ok2 ? (size_t)wi + (size_t)nx * wcy2 + ko : 0), ok2);
-                    }
-                }
-            }
-            asm volatile("cp.async.commit_group;" ::: "memory");
-        };
+        const int P0 = z0 - 2;          // first x plane staged
+        const int XL = z1 + 1, CL = z1; // last x plane, last coefficient plane
+        // slots: x plane p in (p - P0) mod SP_NSX, coefficient plane q in (q - P0) mod SP_NSC.
+        // A commit group holds x plane p and coefficient plane p - 1.
+        auto zin = [&](int t) { return (t >= 0 && t < nz) || L.per_z; };
+        auto zzero = [&](int t) { return t == 0 || (L.per_z && t == nz); }; // plane t is plane 0
         // coarse correction of a pair (both cells share the parent) in plane p
         auto corr = [&](bool in_xy, int ii, int jj, int p) -> T {
             if (!PROL) return (T)0;
@@ -252,98 +168,169 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const S
             if (!in_xy || kz < 0) return (T)0;
             return __ldg(a.e_c + (size_t)(ii >> 1) + (size_t)a.ncx * ((size_t)(jj >> 1) + (size_t)a.ncy * (size_t)(kz >> 1)));
         };
-        // x pair of plane p staged at offset f, with the correction added (and written back for
-        // the other threads when `publish`)
-        auto take = [&](int p, int f, T e, bool publish) -> P2<T> {
-            T* s = &xslot(p).x[0][0] + f;
+        // x pair staged at f of slot sx, with the correction added and written back for the others
+        auto take = [&](int sx, int f, T e) -> P2<T> {
+            T* sp = xs0 + sx * XE + f;
             P2<T> v{(T)0, (T)0};
-            if constexpr (!ZERO) v = sp_ld2<T>(s);
+            if constexpr (!ZERO) v = sp_ld2<T>(sp);
             if constexpr (PROL) {
                 v.a += e;
                 v.b += e;
-                if (publish) sp_st2<T>(s, v.a, v.b);
+                sp_st2<T>(sp, v.a, v.b);
             }
             return v;
         };
-
-        // ---- prologue: x planes P0, P0+1 and the coefficients of plane P0 ----
-#pragma unroll
-        for (int q = 0; q <= SP_D; ++q) issue(P0 + q);
-        asm volatile("cp.async.wait_group %0;" ::"n"(SP_D - 1) : "memory");
-        __syncthreads();
-        P2<T> xprev = take(P0, fx, corr(pin_xy, wi, wj, P0), false);
-        P2<T> xcur = take(P0 + 1, fx, corr(pin_xy, wi, wj, P0 + 1), true);
-        if (has2) (void)take(P0 + 1, fx2, corr(pin2, wi2, wj2, P0 + 1), true);
-        T en = corr(pin_xy, wi, wj, P0 + 2), en2 = has2 ? corr(pin2, wi2, wj2, P0 + 2) : (T)0;
-        P2<T> czp1 = sp_ld2<TC>(&cslot(P0).cz[0][0] + fc); // +z faces of plane t-1 (-z of plane t)
-        P2<T> czp2{(T)0, (T)0};                           // +z faces of plane t-2
-        // carried coefficients of plane t-1 (the black stage)
-        P2<T> b1{}, cx1{}, cy1{}, cyd1{};
-        T cxl1 = 0;
-        T red1 = 0, red2 = 0; // red values of planes t-1 and t-2 in this column
-        double2 r64n = make_double2(0.0, 0.0);
-
-        for (int t = z0 - 1; t <= z1; ++t) {
-            // this thread's copies of x plane t+1 and coefficients of plane t have landed; the
-            // barrier publishes everyone's and the red values of plane t-1, and frees the slots
-            // of x plane t-2 and coefficient plane t-1
-            asm volatile("cp.async.wait_group %0;" ::"n"(SP_D - 2) : "memory");
-            __syncthreads();
-            issue(t + SP_D);
-            const int o = (pj + t) & 1;
-            // ---- x of plane t+1 (own column, and the pairs this thread staged for the others) ----
-            const P2<T> xnext = take(t + 1, fx, en, true);
-            if (has2) (void)take(t + 1, fx2, en2, true);
-            if constexpr (PROL) {
-                en = corr(pin_xy, wi, wj, t + 2);
-                if (has2) en2 = corr(pin2, wi2, wj2, t + 2);
-            }
-            // ---- coefficients of plane t ----
-            const CS& C = cslot(t);
-            const P2<T> b0 = sp_ld2<T>(&C.b[0][0] + fc), cx0 = sp_ld2<TC>(&C.cx[0][0] + fc);
-            const P2<T> cy0 = sp_ld2<TC>(&C.cy[0][0] + fx), cyd0 = sp_ld2<TC>(&C.cy[0][0] + fx - W);
-            const P2<T> cz0 = sp_ld2<TC>(&C.cz[0][0] + fc);
-            const T cxl0 = (T)(&C.cx[0][0])[fc - 1];
-            // ---- red cell pi + o of plane t, from old black values ----
-            T* X0 = &xslot(t).x[0][0];
-            const int kt = wrap_or_out(t, nz, L.per_z);
-            const bool red_in = pin_xy && kt >= 0 && (role != 2 || o != side);
-            T red;
-            {
-                T xin = (T)0, xout = (T)0, xs_ = (T)0, xn_ = (T)0, xt = (T)0, xb = (T)0;
-                if constexpr (!ZERO || PROL) {
-                    xin = xcur.at(1 - o);
-                    xout = X0[fx - 1 + 3 * o];
-                    xs_ = X0[fx - W + o];
-                    xn_ = X0[fx + W + o];
-                    xt = xnext.at(o);
-                    xb = xprev.at(o);
+        // the copies of one pair: x of plane p at fx, b / cx / cy / cz of plane p - 1 (cy at fx,
+        // the others at fx - W); boundary planes wrap (periodic z), are zero, or take the -z faces
+        // bzm for plane -1; `cxb` / `cyb`: the pair is the one left of x = 0 / below y = 0 of a
+        // non-periodic axis, whose cx / cy stand for the boundary faces bxm / bym
+        auto issue_pair = [&](int p, uint32_t xo, uint32_t co, bool pin, long long g, int wi_, int wj_, int fx_,
+                              bool cxb, bool cyb, bool want_x, bool want_c) {
+            const int q = p - 1;
+            const bool dox = !ZERO && want_x && p <= XL, doc = want_c && q >= P0 && q <= CL;
+            if (p >= 1 && p < nz && !cxb && !cyb) { // interior planes: one offset for all arrays
+                const long long off = (g + (long long)nxy * p) * ST;
+                if (dox) sp_cp<2 * ST>(xo + fx_ * ST, reinterpret_cast<const char*>(a.x_in) + (pin ? off : 0), pin);
+                if (doc) {
+                    const long long oq = pin ? off - (long long)nxy * ST : 0;
+                    const uint32_t fcb = co + (fx_ - W) * ST;
+                    sp_cp<2 * ST>(fcb + OB * ST, reinterpret_cast<const char*>(a.b) + oq, pin);
+                    sp_cp<2 * ST>(fcb + OCX * ST, reinterpret_cast<const char*>(L.cx) + oq, pin);
+                    sp_cp<2 * ST>(co + (OCY + fx_) * ST, reinterpret_cast<const char*>(L.cy) + oq, pin);
+                    sp_cp<2 * ST>(fcb + OCZ * ST, reinterpret_cast<const char*>(L.cz) + oq, pin);
                 }
-                const T xw = o ? xin : xout, xe = o ? xout : xin;
-                const T cxp = cx0.at(o), cxm = o ? cx0.a : cxl0;
-                const T cyp = cy0.at(o), cym = cyd0.at(o), czp = cz0.at(o), czm = czp1.at(o);
-                T D = cxm + cxp + cym + cyp + czm + czp;
-                if (L.pin && kt == 0 && wi == 0 && wj == 0 && o == 0) D *= (T)2; // cell 0 is red
-                const T s = cxp * xe + cxm * xw + cyp * xn_ + cym * xs_ + czp * xt + czm * xb;
-                red = red_in ? divide(s - b0.at(o) * dx2, D) : (T)0;
+                return;
             }
-            if (role != 2 || o != side) X0[fx + o] = red;
-            // ---- black cell pi + o of plane t-1 from red values; plane t-1 is then final ----
-            if (role == 0) {
+            T* X = reinterpret_cast<T*>(sp_sm + (xo - xs0_u));
+            T* Cb = reinterpret_cast<T*>(sp_sm + (co - xs0_u));
+            const int fc_ = fx_ - W;
+            if (dox) {
+                const int kz = wrap_or_out(p, nz, L.per_z);
+                const bool ok = pin && kz >= 0;
+                pmv_cp<2 * ST>(X + fx_, a.x_in + (ok ? (size_t)g + nxy * (size_t)kz : 0), ok);
+            }
+            if (doc) {
+                const int kz = wrap_or_out(q, nz, L.per_z);
+                const bool kin = kz >= 0;
+                const bool ok = pin && kin;
+                const size_t gq = ok ? (size_t)g + nxy * (size_t)kz : 0;
+                pmv_cp<2 * ST>(Cb + OB + fc_, a.b + gq, ok);
+                if (cxb) { // -x face of cell (0, wj_): one value into the column of cell -1
+                    const bool okb = wj_ >= 0 && kin;
+                    pmv_cp<ST>(Cb + OCX + fc_ + 1, L.bxm + (okb ? (size_t)wj_ + (size_t)ny * kz : 0), okb);
+                } else {
+                    pmv_cp<2 * ST>(Cb + OCX + fc_, L.cx + gq, ok);
+                }
+                if (cyb) { // -y faces of the pair's cells in row 0
+                    const bool okb = wi_ >= 0 && kin;
+                    pmv_cp<2 * ST>(Cb + OCY + fx_, L.bym + (okb ? (size_t)wi_ + (size_t)nx * kz : 0), okb);
+                } else {
+                    pmv_cp<2 * ST>(Cb + OCY + fx_, L.cy + gq, ok);
+                }
+                if (q == -1 && !L.per_z) { // the -z faces of plane 0 stand in for plane -1's +z faces
+                    pmv_cp<2 * ST>(Cb + OCZ + fc_, L.bzm + (pin ? (size_t)g : 0), pin);
+                } else {
+                    pmv_cp<2 * ST>(Cb + OCZ + fc_, L.cz + gq, ok);
+                }
+            }
+        };
+        int sxi = 0, sci = SP_NSC - 1; // slots of the next group's x plane and coefficient plane
+        // slots of the planes the first step (t = z0 - 1) reads: x t-1, t, t+1; coefficients t
+        int sxm = 0, sx0 = 1, sx1 = 2, sc0 = 1;
+        auto advance = [&]() { // the issue slots advance as the groups are issued
+            sxm = sx0, sx0 = sx1, sx1 = nxs(sx1);
+            sc0 = ncs(sc0);
+        };
+        auto slot_u = [&](int sx, int sc, uint32_t& xo, uint32_t& co) {
+            xo = xs0_u + (uint32_t)(sx * XE * ST);
+            co = cs0_u + (uint32_t)(sc * CE * ST);
+        };
+
+        if (role == 0) {
+            // =============== tile pairs: red of plane t and black of plane t-1 ===============
+            const int pj = j0 + tyr, pi = i0 + 2 * lo;
+            const int wi = pi < nx ? pi : -1, wj = pj < ny ? pj : -1; // never wrapped
+            const bool pin_xy = wi >= 0 && wj >= 0;
+            const long long gxy = pin_xy ? (long long)wi + (long long)nx * wj : 0;
+            const int fx = (pj - j0 + 2) * W + (pi - i0 + 2), fc = fx - W;
+            auto issue = [&](int p) {
+                uint32_t xo, co;
+                slot_u(sxi, sci, xo, co);
+                issue_pair(p, xo, co, pin_xy, gxy, wi, wj, fx, false, false, true, true);
+                asm volatile("cp.async.commit_group;" ::: "memory");
+                sxi = nxs(sxi);
+                sci = ncs(sci);
+            };
+#pragma unroll
+            for (int q = 0; q <= SP_D; ++q) issue(P0 + q);
+            asm volatile("cp.async.wait_group %0;" ::"n"(SP_D - 1) : "memory");
+            asm volatile("bar.sync 0;" ::: "memory");
+            const int wpar = warp & 1; // parity of this warp's rows (j0 is even)
+            const P2<T> xp0 = take(0, fx, corr(pin_xy, wi, wj, P0)); // x(P0): only its own column reads it
+            const P2<T> xp1 = take(1, fx, corr(pin_xy, wi, wj, P0 + 1)); // x(P0 + 1), published
+            T en = corr(pin_xy, wi, wj, P0 + 2); // correction of the pair in plane t + 1
+            P2<T> czp1 = sp_ld2<TC>(cs0 + OCZ + fc), czp2{(T)0, (T)0}; // cz of planes t-1, t-2
+            // carried: A = x(t).at(1-O), B = x(t-1).at(O), the red values of planes t-1 (column
+            // 1-O) and t-2 (column O), the black cell's coefficients of plane t-1 (column O)
+            const int O0 = (wpar + z0 - 1) & 1;
+            T A = O0 ? xp1.a : xp1.b, B = O0 ? xp0.b : xp0.a;
+            T red1 = 0, red2 = 0, kb = 0, kxp = 0, kxm = 0, kyp = 0, kym = 0;
+            double2 r64n = make_double2(0.0, 0.0);
+            T* const xout_base = a.x_out + gxy;
+
+            auto step = [&](auto Oc, int t) {
+                constexpr int O = decltype(Oc)::value;
+                issue(t + SP_D);
+                // ---- x of plane t+1 (own column; published for the neighbours with PROL) ----
+                T xnO;
+                if constexpr (PROL) {
+                    const P2<T> v = take(sx1, fx, en);
+                    xnO = O ? v.b : v.a;
+                    en = corr(pin_xy, wi, wj, t + 2);
+                } else if constexpr (ZERO) {
+                    xnO = (T)0;
+                } else {
+                    xnO = xs0[sx1 * XE + fx + O];
+                }
+                // ---- coefficients of plane t ----
+                const T* C = cs0 + sc0 * CE;
+                const P2<T> b2 = sp_ld2<T>(C + OB + fc), cx2p = sp_ld2<TC>(C + OCX + fc);
+                const P2<T> cy2p = sp_ld2<TC>(C + OCY + fx), cyd2 = sp_ld2<TC>(C + OCY + fx - W);
+                const P2<T> cz2 = sp_ld2<TC>(C + OCZ + fc);
+                const T cxl = (T)C[OCX + fc - 1];
+                // ---- red cell pi + O of plane t, from old black values ----
+                T* X0 = xs0 + sx0 * XE;
+                T red = (T)0;
+                {
+                    T xout = (T)0, xsv = (T)0, xnv = (T)0;
+                    if constexpr (!ZERO || PROL) {
+                        xout = X0[fx - 1 + 3 * O];
+                        xsv = X0[fx - W + O];
+                        xnv = X0[fx + W + O];
+                    }
+                    const T xw = O ? A : xout, xe = O ? xout : A;
+                    const T cxp = O ? cx2p.b : cx2p.a, cxm = O ? cx2p.a : cxl;
+                    const T cyp = O ? cy2p.b : cy2p.a, cym = O ? cyd2.b : cyd2.a;
+                    const T czp = O ? cz2.b : cz2.a, czm = O ? czp1.b : czp1.a;
+                    T D = cxm + cxp + cym + cyp + czm + czp;
+                    if (O == 0 && L.pin && pi == 0 && pj == 0 && zzero(t)) D *= (T)2; // cell 0 is red
+                    const T sum = cxp * xe + cxm * xw + cyp * xnv + cym * xsv + czp * xnO + czm * B;
+                    const T bb = O ? b2.b : b2.a;
+                    if (pin_xy && zin(t)) red = divide(sum - bb * dx2, D);
+                }
+                X0[fx + O] = red;
+                // ---- black cell pi + O of plane t-1 from red values; plane t-1 is then final ----
                 const int q = t - 1;
-                const bool out_q = q >= z0 && q < z1 && pin_xy;
-                if (out_q) {
-                    const T* X1 = &xslot(q).x[0][0];
-                    const T xout = X1[fx - 1 + 3 * o], xs_ = X1[fx - W + o], xn_ = X1[fx + W + o];
-                    const T xw = o ? red1 : xout, xe = o ? xout : red1;
-                    const T cxp = cx1.at(o), cxm = o ? cx1.a : cxl1;
-                    const T cyp = cy1.at(o), cym = cyd1.at(o), czp = czp1.at(o), czm = czp2.at(o);
-                    const T D = cxm + cxp + cym + cyp + czm + czp;
-                    const T s = cxp * xe + cxm * xw + cyp * xn_ + cym * xs_ + czp * red + czm * red2;
-                    const T blk = divide(s - b1.at(o) * dx2, D);
-                    const T va = o ? red1 : blk, vb = o ? blk : red1;
-                    const size_t c = (size_t)gxy + nxy * (size_t)q;
-                    sp_stg2<T>(a.x_out + c, va, vb);
+                if (q >= z0 && q < z1 && pin_xy) {
+                    const T* X1 = xs0 + sxm * XE;
+                    const T xout = X1[fx - 1 + 3 * O], xsv = X1[fx - W + O], xnv = X1[fx + W + O];
+                    const T xw = O ? red1 : xout, xe = O ? xout : red1;
+                    const T kzp = O ? czp1.b : czp1.a, kzm = O ? czp2.b : czp2.a;
+                    const T D = kxm + kxp + kym + kyp + kzm + kzp;
+                    const T sum = kxp * xe + kxm * xw + kyp * xnv + kym * xsv + kzp * red + kzm * red2;
+                    const T blk = divide(sum - kb * dx2, D);
+                    const T va = O ? red1 : blk, vb = O ? blk : red1;
+                    sp_stg2<T>(xout_base + nxy * (size_t)q, va, vb);
                     if constexpr (DOT) dot_acc += r64n.x * (double)va + r64n.y * (double)vb;
                 }
                 if constexpr (DOT) { // r64 of plane t, for the output of plane t at the next step
@@ -351,15 +338,153 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const S
                     r64n = out_t ? __ldg(reinterpret_cast<const double2*>(a.r64 + (size_t)gxy + nxy * (size_t)t))
                                  : make_double2(0.0, 0.0);
                 }
+                // ---- carry to the next plane (red offset 1 - O) ----
+                B = A;
+                A = xnO;
+                red2 = red1;
+                red1 = red;
+                kb = O ? b2.a : b2.b;
+                kxp = O ? cx2p.a : cx2p.b;
+                kxm = O ? cxl : cx2p.a;
+                kyp = O ? cy2p.a : cy2p.b;
+                kym = O ? cyd2.a : cyd2.b;
+                czp2 = czp1;
+                czp1 = cz2;
+            };
+            using Z = std::integral_constant<int, 0>;
+            using I = std::integral_constant<int, 1>;
+            for (int t = z0 - 1; t <= z1; ++t) {
+                // this thread's copies of x plane t+1 and coefficients of plane t have landed; the
+                // barrier publishes everyone's and the red values of plane t-1, and frees the slots
+                // of x plane t-2 and coefficient plane t-1
+                asm volatile("cp.async.wait_group %0;" ::"n"(SP_D - 2) : "memory");
+                asm volatile("bar.sync 0;" ::: "memory");
+                if (((wpar + t) & 1) == 0) step(Z{}, t);
+                else step(I{}, t);
+                advance();
             }
-            // ---- carry to the next plane ----
-            red2 = red1;
-            red1 = red;
-            xprev = xcur;
-            xcur = xnext;
-            b1 = b0, cx1 = cx0, cy1 = cy0, cyd1 = cyd0, cxl1 = cxl0;
-            czp2 = czp1;
-            czp1 = cz0;
+        } else {
+            // =============== ring pairs / cells: red of plane t only ===============
+            int pj, pi, side = -1;
+            if (role == 1) pj = hi ? j0 + SP_TY : j0 - 1, pi = i0 + 2 * lo;
+            else side = hi, pj = j0 + lo, pi = hi ? i0 + SP_TX : i0 - 2;
+            const int wi = wrap_or_out(pi, nx, L.per_x), wj = wrap_or_out(pj, ny, L.per_y);
+            const bool pin_xy = wi >= 0 && wj >= 0;
+            const long long gxy = pin_xy ? (long long)wi + (long long)nx * wj : 0;
+            const int fx = (pj - j0 + 2) * W + (pi - i0 + 2), fc = fx - W;
+            // second x pair: the ring-row warp the outer rows, ring-column lanes 0/1 of each side
+            // the corner pairs (rows j0-1, j0+TY)
+            int sj = 0;
+            bool has2 = false;
+            if (role == 1) has2 = true, sj = hi ? j0 + SP_TY + 1 : j0 - 2;
+            else if (lo == 0 || lo == 1) has2 = true, sj = lo ? j0 + SP_TY : j0 - 1;
+            const int wj2 = wrap_or_out(sj, ny, L.per_y);
+            const bool pin2 = has2 && wi >= 0 && wj2 >= 0;
+            const long long gxy2 = pin2 ? (long long)wi + (long long)nx * wj2 : 0;
+            const int fx2 = (sj - j0 + 2) * W + (pi - i0 + 2);
+            // coefficients beyond the pair's own: cx of the left corner pairs (ring-column lanes
+            // 0 / 1 of the left side: the -x faces of the ring-row cells at i0), cy of the row
+            // below the ring row (ring-row lanes 0-15) and of row j0-1 beside the tile
+            // (ring-column lanes 0 / 16: the -y faces of the ring-column cells at j0)
+            const bool cx2 = role == 2 && side == 0 && has2;
+            const bool cy2 = (role == 1 && !hi) || (role == 2 && lo == 0);
+            const int cy2j = role == 1 ? j0 - 2 : j0 - 1;
+            const int wcy2 = wrap_or_out(cy2j, ny, L.per_y);
+            const bool cx_bnd = pi == -2 && !L.per_x, cy_bnd = pj == -1 && !L.per_y;
+            const bool cy2_bnd = cy2j == -1 && !L.per_y;
+            const long long gcy2 = (wi >= 0 && wcy2 >= 0) ? (long long)wi + (long long)nx * wcy2 : 0;
+            const int fyy = (cy2j - j0 + 2) * W + (pi - i0 + 2);
+            auto issue = [&](int p) {
+                uint32_t xo, co;
+                slot_u(sxi, sci, xo, co);
+                issue_pair(p, xo, co, pin_xy, gxy, wi, wj, fx, cx_bnd, cy_bnd, true, true);
+                if (has2) { // x of the second pair; cx of a corner pair
+                    issue_pair(p, xo, co, pin2, gxy2, wi, wj2, fx2, false, false, true, false);
+                    if (cx2) { // only cx of plane p - 1 (b, cy, cz of the corner are not read)
+                        const int q = p - 1;
+                        if (q >= P0 && q <= CL) {
+                            T* Cb = reinterpret_cast<T*>(sp_sm + (co - xs0_u));
+                            const int kz = wrap_or_out(q, nz, L.per_z);
+                            const bool kin = kz >= 0;
+                            if (cx_bnd) {
+                                const bool okb = wj2 >= 0 && kin;
+                                pmv_cp<ST>(Cb + OCX + fx2 - W + 1, L.bxm + (okb ? (size_t)wj2 + (size_t)ny * kz : 0), okb);
+                            } else {
+                                const bool ok2 = pin2 && kin;
+                                pmv_cp<2 * ST>(Cb + OCX + fx2 - W,
+                                               L.cx + (ok2 ? (size_t)gxy2 + nxy * (size_t)kz : 0), ok2);
+                            }
+                        }
+                    }
+                }
+                if (cy2) { // cy of plane p - 1 in row cy2j
+                    const int q = p - 1;
+                    if (q >= P0 && q <= CL) {
+                        T* Cb = reinterpret_cast<T*>(sp_sm + (co - xs0_u));
+                        const int kz = wrap_or_out(q, nz, L.per_z);
+                        const bool kin = kz >= 0;
+                        if (cy2_bnd) {
+                            const bool okb = wi >= 0 && kin;
+                            pmv_cp<2 * ST>(Cb + OCY + fyy, L.bym + (okb ? (size_t)wi + (size_t)nx * kz : 0), okb);
+                        } else {
+                            const bool ok2 = wi >= 0 && wcy2 >= 0 && kin;
+                            pmv_cp<2 * ST>(Cb + OCY + fyy, L.cy + (ok2 ? (size_t)gcy2 + nxy * (size_t)kz : 0), ok2);
+                        }
+                    }
+                }
+                asm volatile("cp.async.commit_group;" ::: "memory");
+                sxi = nxs(sxi);
+                sci = ncs(sci);
+            };
+#pragma unroll
+            for (int q = 0; q <= SP_D; ++q) issue(P0 + q);
+            asm volatile("cp.async.wait_group %0;" ::"n"(SP_D - 1) : "memory");
+            asm volatile("bar.sync 0;" ::: "memory");
+            P2<T> xprev = take(0, fx, corr(pin_xy, wi, wj, P0));
+            P2<T> xcur = take(1, fx, corr(pin_xy, wi, wj, P0 + 1));
+            if (has2) (void)take(1, fx2, corr(pin2, wi, wj2, P0 + 1));
+            T en = corr(pin_xy, wi, wj, P0 + 2), en2 = has2 ? corr(pin2, wi, wj2, P0 + 2) : (T)0;
+            P2<T> czp1 = sp_ld2<TC>(cs0 + OCZ + fc);
+            for (int t = z0 - 1; t <= z1; ++t) {
+                asm volatile("cp.async.wait_group %0;" ::"n"(SP_D - 2) : "memory");
+                asm volatile("bar.sync 0;" ::: "memory");
+                issue(t + SP_D);
+                const int o = (pj + t) & 1;
+                const P2<T> xnext = take(sx1, fx, en);
+                if (has2) (void)take(sx1, fx2, en2);
+                if constexpr (PROL) {
+                    en = corr(pin_xy, wi, wj, t + 2);
+                    if (has2) en2 = corr(pin2, wi, wj2, t + 2);
+                }
+                const T* C = cs0 + sc0 * CE;
+                const P2<T> b2 = sp_ld2<T>(C + OB + fc), cx2p = sp_ld2<TC>(C + OCX + fc);
+                const P2<T> cy2p = sp_ld2<TC>(C + OCY + fx), cyd2 = sp_ld2<TC>(C + OCY + fx - W);
+                const P2<T> cz2 = sp_ld2<TC>(C + OCZ + fc);
+                const T cxl = (T)C[OCX + fc - 1];
+                T* X0 = xs0 + sx0 * XE;
+                if (role == 1 || o != side) { // a ring-column cell is relaxed where it is red
+                    T xout = (T)0, xsv = (T)0, xnv = (T)0;
+                    if constexpr (!ZERO || PROL) {
+                        xout = X0[fx - 1 + 3 * o];
+                        xsv = X0[fx - W + o];
+                        xnv = X0[fx + W + o];
+                    }
+                    const T xin = xcur.at(1 - o);
+                    const T xw = o ? xin : xout, xe = o ? xout : xin;
+                    const T cxp = cx2p.at(o), cxm = o ? cx2p.a : cxl;
+                    const T cyp = cy2p.at(o), cym = cyd2.at(o), czp = cz2.at(o), czm = czp1.at(o);
+                    T D = cxm + cxp + cym + cyp + czm + czp;
+                    if (L.pin && wi == 0 && wj == 0 && o == 0 && zzero(t)) D *= (T)2;
+                    const T sum = cxp * xe + cxm * xw + cyp * xnv + cym * xsv + czp * xnext.at(o) + czm * xprev.at(o);
+                    T red = (T)0;
+                    if (pin_xy && zin(t)) red = divide(sum - b2.at(o) * dx2, D);
+                    X0[fx + o] = red;
+                }
+                xprev = xcur;
+                xcur = xnext;
+                czp1 = cz2;
+                advance();
+            }
         }
         asm volatile("cp.async.wait_all;" ::: "memory");
     }

@@ -84,6 +84,9 @@ PAIR_CASES = [
     ((40, 18, 34), [D, D, N, N, N, N], [1.0, 0.0, 0, 0, 0, 0], False),
     ((5, 3, 2), [D] * 6, [1.0, 0.0, 0.2, 0.4, 0.6, 0.8], False),
     ((96, 48, 96), [D, D, N, N, N, N], [1.0, 0.0, 0, 0, 0, 0], False),
+    # 64 tiles: z chunks of several planes, so that the steady-state staging runs
+    ((64, 128, 256), [D, D, N, N, N, N], [1.0, 0.0, 0, 0, 0, 0], False),
+    ((48, 128, 128), [D, D, P, P, N, N], [1.0, 0.0, 0, 0, 0, 0], False),
 ]
 
 
