@@ -7,49 +7,53 @@
 // summed for the preconditioned CG (M_DOT).
 //
 // Schedule.  A CTA owns a 32 x 16 column tile and marches a z chunk [z0, z1).  Every thread of
-// the 8 tile warps owns an x-pair of cells (2m, 2m+1) of one row.  In plane t the red cell of
-// the pair is 2m + o with o = (j + t) & 1; in plane t-1 the same column holds a black cell.  At
-// step t the thread therefore
+// the 8 tile warps owns an x-pair of cells (2m, 2m+1) of one row (a warp covers rows r and
+// r+2, so the red offset is the same for the whole warp).  In plane t the red cell of the pair
+// is 2m + O with O = (j + t) & 1; in plane t-1 the same column holds a black cell.  At step t
+// the thread therefore
 //   - relaxes its red cell of plane t from old black values,
 //   - relaxes the black cell of plane t-1 in the same column from the red values of planes
 //     t-2, t-1 (published at the previous step) and t (just computed),
 //   - writes plane t-1, now final, as one pair (red value of the last step, black value now).
 // Only red values go through shared memory (one store per thread and step); a thread keeps
 // the old x of its own column for planes t-1 .. t+1, its last two red values and the
-// coefficient pairs of the last plane in registers.  ONE barrier per plane.
+// coefficients of the last plane in registers.  ONE barrier per plane.
 //
 // The black updates next to the tile need the red values of the one-cell ring around it, so
 // two more warps relax the red cells of that ring (without storing them): warp 8 the ring
 // rows below and above the tile (x-pairs), warp 9 the ring columns left and right (one cell
 // each, relaxed in the planes where it is red).  x is staged with a two-cell ring for them.
 //
-// Periodic axes must be a whole number of tiles (x: 32 cells, y: 16), so that the ring of a
-// tile is the wrapped neighbour of its edge.
-//
-// Staging.  Every thread copies, by cp.async into rings of shared-memory slots, the x pair(s)
-// it owns and their b / face coefficients; the ring warps also stage the outer x rows, the
-// corner pairs and the boundary faces the tile needs.  x plane p and the coefficients of
-// plane p - 1 form one commit group, issued SP_D planes ahead, so the coefficients arrive
-// exactly one step before their use.  Cells beyond a non-periodic face are staged as zeros
-// (the ghost value); the -x / -y / -z faces of the first cells come from the boundary-face
-// planes bxm / bym / bzm; periodic axes wrap.  With M_PROLONG the stager adds the coarse
-// correction to the pairs it staged before the barrier that publishes them.
+// Staging, two forms (template parameter TM):
+//   TMA (non-periodic grids whose rows are 16-byte multiples): one thread copies each plane's
+//     x box and coefficient boxes (tile plus ring, zero-filled beyond the grid: the ghost
+//     value) with cp.async.bulk.tensor, and the -x / -y / -z boundary faces of the first cells
+//     from the boundary-face planes bxm / bym / bzm; one full mbarrier per group, waited on by
+//     that thread (bounded) before the step barrier.
+//   cp.async (periodic axes, which must then be a whole number of tiles): every thread copies
+//     its own x pair(s) and their coefficients; the ring warps also stage the outer rows,
+//     corners and boundary faces; wrapped coordinates on periodic axes.
+// x plane p and the coefficients of plane p - 1 form one group, issued SP_D planes ahead, so
+// the coefficients arrive one step before their use.  With M_PROLONG each thread adds the
+// coarse correction to the pairs it owns (and the ring warps to the outer pairs) before the
+// barrier that publishes them.
 #pragma once
+#include <cuda.h>
+
 #include <cstddef>
 #include <type_traits>
 
 #include "kernels_mg.cuh"
 #include "kernels_pcg.cuh"
+#include "kernels_sweep_tma.cuh"
 
 namespace mf3d {
 
-constexpr int SP_TX = 32, SP_TY = 16;     // tile (cells)
-constexpr int SP_PX = SP_TX / 2;          // pairs per tile row
-constexpr int SP_W = SP_TX + 4;           // slot row pitch: columns i0-2 .. i0+TX+1
-constexpr int SP_XR = SP_TY + 4;          // x rows j0-2 .. j0+TY+1
-constexpr int SP_CR = SP_TY + 2;          // b, cx, cz rows j0-1 .. j0+TY
-constexpr int SP_YR = SP_TY + 3;          // cy rows j0-2 .. j0+TY
-constexpr int SP_NT = 320;                // 8 tile warps + ring rows + ring columns
+constexpr int SP_TX = 32, SP_TY = 16; // tile (cells)
+constexpr int SP_XR = SP_TY + 4;      // x rows j0-2 .. j0+TY+1
+constexpr int SP_CR = SP_TY + 2;      // b, cx, cz rows j0-1 .. j0+TY
+constexpr int SP_YR = SP_TY + 3;      // cy rows j0-2 .. j0+TY
+constexpr int SP_NT = 320;            // 8 tile warps + ring rows + ring columns
 #ifndef MF3D_SP_D
 #define MF3D_SP_D 3 // planes staged ahead of the one the red stage reads
 #endif
@@ -57,18 +61,25 @@ constexpr int SP_D = MF3D_SP_D;
 constexpr int SP_NSX = SP_D + 2; // x planes t-1 .. t+D
 constexpr int SP_NSC = SP_D;     // coefficient planes t .. t+D-1
 
-template <class T> struct SpXSlot {
-    T x[SP_XR][SP_W];
+// Shared-memory layout of one precision and staging form.  Columns i0-HX .. i0+TX+HX-1 (a TMA
+// box starts on a 16-byte boundary); every array of a slot starts on a 128-byte boundary.
+template <class T, bool TM> struct SpGeom {
+    static constexpr int ST = (int)sizeof(T);
+    static constexpr int HX = TM ? 16 / ST : 2;
+    static constexpr int W = SP_TX + 2 * HX;
+    static constexpr int BXS = TM ? 16 / ST : 2; // the -x face buffer starts at row j0 - BXS
+    static constexpr int BXN = SP_TY + 2 * BXS;
+    static constexpr size_t a128(size_t v) { return (v + 127) & ~(size_t)127; }
+    static constexpr size_t XSB = a128((size_t)SP_XR * W * ST); // x slot
+    static constexpr size_t CB = a128((size_t)SP_CR * W * ST), CYB = a128((size_t)SP_YR * W * ST);
+    // coefficient slot: b, cx, cy, cz, then the -x faces (bxm) and -y faces (bym) of a tile on
+    // the grid's min faces (TMA form)
+    static constexpr size_t OB = 0, OCX = CB, OCY = 2 * CB, OCZ = 2 * CB + CYB, OBX = 3 * CB + CYB;
+    static constexpr size_t OBY = OBX + a128((size_t)BXN * ST);
+    static constexpr size_t CSB = OBY + a128((size_t)W * ST);
+    static constexpr size_t SMEM = SP_NSX * XSB + SP_NSC * CSB + 128; // + alignment of the base
 };
-template <class T, class TC> struct SpCSlot {
-    T b[SP_CR][SP_W];
-    TC cx[SP_CR][SP_W];
-    TC cy[SP_YR][SP_W];
-    TC cz[SP_CR][SP_W];
-};
-template <class T, class TC> constexpr size_t sp_smem_bytes() {
-    return SP_NSX * sizeof(SpXSlot<T>) + SP_NSC * sizeof(SpCSlot<T, TC>);
-}
+template <class T, class TC, bool TM> constexpr size_t sp_smem_bytes() { return SpGeom<T, TM>::SMEM; }
 // resident CTAs per SM the register budget is cut for
 template <class T> constexpr int sp_minb() { return sizeof(T) == 8 ? 2 : 3; }
 
@@ -84,6 +95,13 @@ template <class T, class TC> struct SpArgs {
     unsigned* dot_ticket;
     double* dot_out;
     int zchunk; // planes per work item
+    int* err;   // set to 1 when a staging wait gives up (TMA form)
+};
+
+// Tensor maps of the TMA form: x / b / cx / cz / cy boxes of W x (XR | CR | CR | CR | YR) x 1;
+// bxm (ny x nz) box BXN x 1, bym (nx x nz) box W x 1, bzm (nx x ny) box W x CR.
+struct SpMaps {
+    CUtensorMap x, b, cx, cy, cz, bxm, bym, bzm;
 };
 
 template <class T> struct P2 {
@@ -103,31 +121,39 @@ template <class T> __device__ __forceinline__ void sp_st2(T* p, T a, T b) {
     if constexpr (sizeof(T) == 8) *reinterpret_cast<double2*>(p) = make_double2(a, b);
     else *reinterpret_cast<float2*>(p) = make_float2(a, b);
 }
-template <class T> __device__ __forceinline__ void sp_stg2(T* p, T a, T b) {
-    if constexpr (sizeof(T) == 8) *reinterpret_cast<double2*>(p) = make_double2(a, b);
-    else *reinterpret_cast<float2*>(p) = make_float2(a, b);
-}
+template <class T> __device__ __forceinline__ void sp_stg2(T* p, T a, T b) { sp_st2<T>(p, a, b); }
 
-// cp.async of B bytes (4, 8 or 16) to a shared address; `ok` false reads nothing and zero-fills
+// cp.async of B bytes (4, 8 or 16) to a shared address; `ok` false reads nothing and zero-fills.
+// 16-byte copies bypass L1 (.cg): staged data is never re-read through L1, and allocating it
+// there measured 1.5x slower (FP64 plain sweep at 256^3: 0.363 ms with .ca, 0.246 ms with .cg).
 template <int B> __device__ __forceinline__ void sp_cp(uint32_t dst, const char* src, bool ok) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(dst), "l"(src), "n"(B), "r"(ok ? B : 0)
-                 : "memory");
+    if constexpr (B == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], %2, %3;" ::"r"(dst), "l"(src), "n"(B), "r"(ok ? B : 0)
+                     : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(dst), "l"(src), "n"(B), "r"(ok ? B : 0)
+                     : "memory");
 }
 
-template <class T, class TC, int MODE>
-__global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const SpArgs<T, TC> a) {
+template <class T, class TC, int MODE, bool TM>
+__global__ void __launch_bounds__(SP_NT, sp_minb<T>())
+    sweep_pair_kernel(const __grid_constant__ SpMaps maps, const SpArgs<T, TC> a) {
     static_assert(sizeof(T) == sizeof(TC) && sizeof(T) >= 4, "FP64 or FP32 vectors with coefficients of the same type");
     constexpr bool ZERO = (MODE & M_ZERO) != 0, PROL = (MODE & M_PROLONG) != 0, DOT = (MODE & M_DOT) != 0;
     static_assert((MODE & M_RESID) == 0, "the residual runs in a kernel of its own");
-    constexpr int ST = (int)sizeof(T), W = SP_W;
-    using XS = SpXSlot<T>;
-    using CS = SpCSlot<T, TC>;
-    extern __shared__ __align__(16) unsigned char sp_sm[];
-    T* const xs0 = reinterpret_cast<T*>(sp_sm); // x slot s starts at xs0 + s * XE
-    constexpr int XE = (int)(sizeof(XS) / sizeof(T));
-    constexpr int CE = (int)(sizeof(CS) / sizeof(T));
-    T* const cs0 = reinterpret_cast<T*>(sp_sm + SP_NSX * sizeof(XS)); // coefficient slot s at cs0 + s * CE
-    constexpr int OB = 0, OCX = SP_CR * W, OCY = 2 * SP_CR * W, OCZ = 2 * SP_CR * W + SP_YR * W; // arrays in a slot
+    using G = SpGeom<T, TM>;
+    constexpr int ST = G::ST, W = G::W, HX = G::HX;
+    extern __shared__ __align__(128) unsigned char sp_sm_raw[];
+    // slots start on a 128-byte boundary of the shared window (TMA destinations)
+    unsigned char* const sp_sm =
+        sp_sm_raw + ((128u - ((uint32_t)__cvta_generic_to_shared(sp_sm_raw) & 127u)) & 127u);
+    __shared__ __align__(8) uint64_t sp_full[SP_NSX]; // TMA form: one full barrier per group (x slot)
+    T* const xs0 = reinterpret_cast<T*>(sp_sm); // x slot s at xs0 + s * XE
+    constexpr int XE = (int)(G::XSB / ST), CE = (int)(G::CSB / ST);
+    T* const cs0 = reinterpret_cast<T*>(sp_sm + SP_NSX * G::XSB); // coefficient slot s at cs0 + s * CE
+    // arrays in a coefficient slot, in elements
+    constexpr int OB = (int)(G::OB / ST), OCX = (int)(G::OCX / ST), OCY = (int)(G::OCY / ST);
+    constexpr int OCZ = (int)(G::OCZ / ST), OBX = (int)(G::OBX / ST), OBY = (int)(G::OBY / ST);
     const uint32_t xs0_u = (uint32_t)__cvta_generic_to_shared(xs0), cs0_u = (uint32_t)__cvta_generic_to_shared(cs0);
 
     const LevelOp<TC>& L = a.L;
@@ -149,16 +175,27 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const S
     auto nxs = [](int s) { return s + 1 == SP_NSX ? 0 : s + 1; };
     auto ncs = [](int s) { return s + 1 == SP_NSC ? 0 : s + 1; };
     double dot_acc = 0.0;
+    // TMA form: thread 0 issues every copy and waits on the groups' barriers
+    unsigned phase = 0u; // thread 0: parity of the next wait, per barrier
+    bool fail = false;
+    if constexpr (TM) {
+        if (tid == 0) {
+            for (int k = 0; k < SP_NSX; ++k) mbar_init(&sp_full[k], 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+    }
 
-    for (int item = blockIdx.x; item < total; item += gridDim.x) {
-        __syncthreads(); // the previous item's reads of the slots are done
+    for (int item = blockIdx.x; item < total && !fail; item += gridDim.x) {
+        if constexpr (TM) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads(); // the previous item's reads (and generic writes) of the slots are done
         const int tile = item % ntiles;
         const int z0 = (item / ntiles) * a.zchunk, z1 = min(z0 + a.zchunk, nz);
         const int i0 = (tile % ntx) * SP_TX, j0 = (tile / ntx) * SP_TY;
         const int P0 = z0 - 2;          // first x plane staged
         const int XL = z1 + 1, CL = z1; // last x plane, last coefficient plane
         // slots: x plane p in (p - P0) mod SP_NSX, coefficient plane q in (q - P0) mod SP_NSC.
-        // A commit group holds x plane p and coefficient plane p - 1.
+        // A group holds x plane p and coefficient plane p - 1; it is empty past both ends.
+        auto real = [&](int p) { return (!ZERO && p <= XL) || (p - 1 >= P0 && p - 1 <= CL); };
         auto zin = [&](int t) { return (t >= 0 && t < nz) || L.per_z; };
         auto zzero = [&](int t) { return t == 0 || (L.per_z && t == nz); }; // plane t is plane 0
         // coarse correction of a pair (both cells share the parent) in plane p
@@ -179,6 +216,98 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const S
                 sp_st2<T>(sp, v.a, v.b);
             }
             return v;
+        };
+        int sxi = 0, sci = SP_NSC - 1; // slots of the next group's x plane and coefficient plane
+        int next_wait = P0;            // thread 0 (TMA form): the next group to wait for
+        // slots of the planes the first step (t = z0 - 1) reads: x t-1, t, t+1; coefficients t
+        int sxm = 0, sx0 = 1, sx1 = 2, sc0 = 1;
+        auto advance = [&]() { // the issue slots advance as the groups are issued
+            sxm = sx0, sx0 = sx1, sx1 = nxs(sx1);
+            sc0 = ncs(sc0);
+        };
+        // ---- TMA form: thread 0's copies of group p and its waits ----
+        auto tma_issue = [&](int p) {
+            if constexpr (TM) {
+                if (tid == 0 && real(p)) {
+                    const int q = p - 1;
+                    const bool dox = !ZERO && p <= XL, doc = q >= P0 && q <= CL;
+                    uint64_t* bar = &sp_full[sxi];
+                    unsigned bytes = 0;
+                    if (dox) bytes += (unsigned)(SP_XR * W * ST);
+                    if (doc) bytes += (unsigned)((3 * SP_CR + SP_YR) * W * ST + (i0 == 0 ? G::BXN * ST : 0) +
+                                                 (j0 == 0 ? W * ST : 0));
+                    mbar_expect_tx(bar, bytes);
+                    if (dox) tma_load_3d(xs0 + sxi * XE, &maps.x, i0 - HX, j0 - 2, p, bar);
+                    if (doc) {
+                        T* C = cs0 + sci * CE;
+                        tma_load_3d(C + OB, &maps.b, i0 - HX, j0 - 1, q, bar);
+                        tma_load_3d(C + OCX, &maps.cx, i0 - HX, j0 - 1, q, bar);
+                        tma_load_3d(C + OCY, &maps.cy, i0 - HX, j0 - 2, q, bar);
+                        if (q == -1) // the -z faces of plane 0 stand in for plane -1's +z faces
+                            tma_load_2d(C + OCZ, &maps.bzm, i0 - HX, j0 - 1, bar);
+                        else
+                            tma_load_3d(C + OCZ, &maps.cz, i0 - HX, j0 - 1, q, bar);
+                        if (i0 == 0) tma_load_2d(C + OBX, &maps.bxm, j0 - G::BXS, q, bar);
+                        if (j0 == 0) tma_load_2d(C + OBY, &maps.bym, i0 - HX, q, bar);
+                    }
+                }
+            }
+        };
+        // thread 0 waits for group p (x slot s); the barrier publishes it (and this step's red
+        // values); false when a wait gave up
+        auto sync_step = [&](int p, int s) -> bool {
+            if constexpr (TM) {
+                bool bad = false;
+                if (tid == 0 && real(p)) {
+                    bad = !mbar_wait(&sp_full[s], (phase >> s) & 1u);
+                    if (!bad) phase ^= 1u << s;
+                }
+                if (tid == 0 && !bad) next_wait = p + 1;
+                // generic writes to the slots (red values, corrections) before later TMA writes
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                return !bar_red_or(1, SP_NT, bad);
+            } else {
+                asm volatile("cp.async.wait_group %0;" ::"n"(SP_D - 2) : "memory");
+                asm volatile("bar.sync 0;" ::: "memory");
+                return true;
+            }
+        };
+        // the first two groups (x planes P0, P0 + 1, coefficients of plane P0)
+        auto sync_prologue = [&]() -> bool {
+            if constexpr (TM) {
+                bool bad = false;
+                if (tid == 0) {
+                    for (int p = P0; p <= P0 + 1 && !bad; ++p) {
+                        if (real(p)) {
+                            const int s = p - P0;
+                            bad = !mbar_wait(&sp_full[s], (phase >> s) & 1u);
+                            if (bad) break;
+                            phase ^= 1u << s;
+                        }
+                        next_wait = p + 1;
+                    }
+                }
+                return !bar_red_or(1, SP_NT, bad);
+            } else {
+                asm volatile("cp.async.wait_group %0;" ::"n"(SP_D - 1) : "memory");
+                asm volatile("bar.sync 0;" ::: "memory");
+                return true;
+            }
+        };
+        // after a failed wait: thread 0 waits (bounded) for the groups it issued and nobody
+        // waited for yet, so that no copy is in flight when the CTA leaves
+        auto drain = [&](int p_last) {
+            if constexpr (TM) {
+                if (tid == 0) {
+                    atomicExch(a.err, 1);
+                    for (int p = next_wait; p <= p_last; ++p) {
+                        if (!real(p)) continue;
+                        const int s = (p - P0) % SP_NSX;
+                        (void)mbar_wait(&sp_full[s], (phase >> s) & 1u);
+                        phase ^= 1u << s;
+                    }
+                }
+            }
         };
         // the copies of one pair: x of plane p at fx, b / cx / cy / cz of plane p - 1 (cy at fx,
         // the others at fx - W); boundary planes wrap (periodic z), are zero, or take the -z faces
@@ -203,6 +332,7 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const S
             }
             T* X = reinterpret_cast<T*>(sp_sm + (xo - xs0_u));
             T* Cb = reinterpret_cast<T*>(sp_sm + (co - xs0_u));
+            // (boundary planes and boundary tiles only: the L1-allocating copy is fine here)
             const int fc_ = fx_ - W;
             if (dox) {
                 const int kz = wrap_or_out(p, nz, L.per_z);
@@ -234,13 +364,6 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const S
                 }
             }
         };
-        int sxi = 0, sci = SP_NSC - 1; // slots of the next group's x plane and coefficient plane
-        // slots of the planes the first step (t = z0 - 1) reads: x t-1, t, t+1; coefficients t
-        int sxm = 0, sx0 = 1, sx1 = 2, sc0 = 1;
-        auto advance = [&]() { // the issue slots advance as the groups are issued
-            sxm = sx0, sx0 = sx1, sx1 = nxs(sx1);
-            sc0 = ncs(sc0);
-        };
         auto slot_u = [&](int sx, int sc, uint32_t& xo, uint32_t& co) {
             xo = xs0_u + (uint32_t)(sx * XE * ST);
             co = cs0_u + (uint32_t)(sc * CE * ST);
@@ -252,19 +375,30 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const S
             const int wi = pi < nx ? pi : -1, wj = pj < ny ? pj : -1; // never wrapped
             const bool pin_xy = wi >= 0 && wj >= 0;
             const long long gxy = pin_xy ? (long long)wi + (long long)nx * wj : 0;
-            const int fx = (pj - j0 + 2) * W + (pi - i0 + 2), fc = fx - W;
+            const int fx = (pj - j0 + 2) * W + (pi - i0 + HX), fc = fx - W;
+            // the -x face of cell pi - 1 and the -y faces of the pair: from the boundary-face
+            // buffers where the TMA form stages them, else from the cx / cy slots
+            const int cxl_off = (TM && i0 == 0 && pi == 0) ? OBX + (pj - j0 + G::BXS) : OCX + fc - 1;
+            const int cyd_off = (TM && j0 == 0 && pj == 0) ? OBY + (pi - i0 + HX) : OCY + fx - W;
             auto issue = [&](int p) {
-                uint32_t xo, co;
-                slot_u(sxi, sci, xo, co);
-                issue_pair(p, xo, co, pin_xy, gxy, wi, wj, fx, false, false, true, true);
-                asm volatile("cp.async.commit_group;" ::: "memory");
+                if constexpr (TM) {
+                    tma_issue(p);
+                } else {
+                    uint32_t xo, co;
+                    slot_u(sxi, sci, xo, co);
+                    issue_pair(p, xo, co, pin_xy, gxy, wi, wj, fx, false, false, true, true);
+                    asm volatile("cp.async.commit_group;" ::: "memory");
+                }
                 sxi = nxs(sxi);
                 sci = ncs(sci);
             };
 #pragma unroll
             for (int q = 0; q <= SP_D; ++q) issue(P0 + q);
-            asm volatile("cp.async.wait_group %0;" ::"n"(SP_D - 1) : "memory");
-            asm volatile("bar.sync 0;" ::: "memory");
+            if (!sync_prologue()) {
+                drain(P0 + SP_D);
+                fail = true;
+                break;
+            }
             const int wpar = warp & 1; // parity of this warp's rows (j0 is even)
             const P2<T> xp0 = take(0, fx, corr(pin_xy, wi, wj, P0)); // x(P0): only its own column reads it
             const P2<T> xp1 = take(1, fx, corr(pin_xy, wi, wj, P0 + 1)); // x(P0 + 1), published
@@ -295,9 +429,9 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const S
                 // ---- coefficients of plane t ----
                 const T* C = cs0 + sc0 * CE;
                 const P2<T> b2 = sp_ld2<T>(C + OB + fc), cx2p = sp_ld2<TC>(C + OCX + fc);
-                const P2<T> cy2p = sp_ld2<TC>(C + OCY + fx), cyd2 = sp_ld2<TC>(C + OCY + fx - W);
+                const P2<T> cy2p = sp_ld2<TC>(C + OCY + fx), cyd2 = sp_ld2<TC>(C + cyd_off);
                 const P2<T> cz2 = sp_ld2<TC>(C + OCZ + fc);
-                const T cxl = (T)C[OCX + fc - 1];
+                const T cxl = (T)C[cxl_off];
                 // ---- red cell pi + O of plane t, from old black values ----
                 T* X0 = xs0 + sx0 * XE;
                 T red = (T)0;
@@ -354,11 +488,14 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const S
             using Z = std::integral_constant<int, 0>;
             using I = std::integral_constant<int, 1>;
             for (int t = z0 - 1; t <= z1; ++t) {
-                // this thread's copies of x plane t+1 and coefficients of plane t have landed; the
-                // barrier publishes everyone's and the red values of plane t-1, and frees the slots
-                // of x plane t-2 and coefficient plane t-1
-                asm volatile("cp.async.wait_group %0;" ::"n"(SP_D - 2) : "memory");
-                asm volatile("bar.sync 0;" ::: "memory");
+                // x plane t+1 and the coefficients of plane t have landed; the barrier publishes
+                // them and the red values of plane t-1, and frees the slots of x plane t-2 and
+                // coefficient plane t-1
+                if (!sync_step(t + 1, sx1)) {
+                    drain(t + SP_D - 1);
+                    fail = true;
+                    break;
+                }
                 if (((wpar + t) & 1) == 0) step(Z{}, t);
                 else step(I{}, t);
                 advance();
@@ -371,7 +508,9 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const S
             const int wi = wrap_or_out(pi, nx, L.per_x), wj = wrap_or_out(pj, ny, L.per_y);
             const bool pin_xy = wi >= 0 && wj >= 0;
             const long long gxy = pin_xy ? (long long)wi + (long long)nx * wj : 0;
-            const int fx = (pj - j0 + 2) * W + (pi - i0 + 2), fc = fx - W;
+            const int fx = (pj - j0 + 2) * W + (pi - i0 + HX), fc = fx - W;
+            const int cxl_off = (TM && i0 == 0 && pi == 0) ? OBX + (pj - j0 + G::BXS) : OCX + fc - 1;
+            const int cyd_off = (TM && j0 == 0 && pj == 0) ? OBY + (pi - i0 + HX) : OCY + fx - W;
             // second x pair: the ring-row warp the outer rows, ring-column lanes 0/1 of each side
             // the corner pairs (rows j0-1, j0+TY)
             int sj = 0;
@@ -381,7 +520,7 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const S
             const int wj2 = wrap_or_out(sj, ny, L.per_y);
             const bool pin2 = has2 && wi >= 0 && wj2 >= 0;
             const long long gxy2 = pin2 ? (long long)wi + (long long)nx * wj2 : 0;
-            const int fx2 = (sj - j0 + 2) * W + (pi - i0 + 2);
+            const int fx2 = (sj - j0 + 2) * W + (pi - i0 + HX);
             // coefficients beyond the pair's own: cx of the left corner pairs (ring-column lanes
             // 0 / 1 of the left side: the -x faces of the ring-row cells at i0), cy of the row
             // below the ring row (ring-row lanes 0-15) and of row j0-1 beside the tile
@@ -393,8 +532,13 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const S
             const bool cx_bnd = pi == -2 && !L.per_x, cy_bnd = pj == -1 && !L.per_y;
             const bool cy2_bnd = cy2j == -1 && !L.per_y;
             const long long gcy2 = (wi >= 0 && wcy2 >= 0) ? (long long)wi + (long long)nx * wcy2 : 0;
-            const int fyy = (cy2j - j0 + 2) * W + (pi - i0 + 2);
+            const int fyy = (cy2j - j0 + 2) * W + (pi - i0 + HX);
             auto issue = [&](int p) {
+                if constexpr (TM) { // thread 0 stages everything
+                    sxi = nxs(sxi);
+                    sci = ncs(sci);
+                    return;
+                }
                 uint32_t xo, co;
                 slot_u(sxi, sci, xo, co);
                 issue_pair(p, xo, co, pin_xy, gxy, wi, wj, fx, cx_bnd, cy_bnd, true, true);
@@ -438,16 +582,20 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const S
             };
 #pragma unroll
             for (int q = 0; q <= SP_D; ++q) issue(P0 + q);
-            asm volatile("cp.async.wait_group %0;" ::"n"(SP_D - 1) : "memory");
-            asm volatile("bar.sync 0;" ::: "memory");
+            if (!sync_prologue()) {
+                fail = true;
+                break;
+            }
             P2<T> xprev = take(0, fx, corr(pin_xy, wi, wj, P0));
             P2<T> xcur = take(1, fx, corr(pin_xy, wi, wj, P0 + 1));
             if (has2) (void)take(1, fx2, corr(pin2, wi, wj2, P0 + 1));
             T en = corr(pin_xy, wi, wj, P0 + 2), en2 = has2 ? corr(pin2, wi, wj2, P0 + 2) : (T)0;
             P2<T> czp1 = sp_ld2<TC>(cs0 + OCZ + fc);
             for (int t = z0 - 1; t <= z1; ++t) {
-                asm volatile("cp.async.wait_group %0;" ::"n"(SP_D - 2) : "memory");
-                asm volatile("bar.sync 0;" ::: "memory");
+                if (!sync_step(t + 1, sx1)) {
+                    fail = true;
+                    break;
+                }
                 issue(t + SP_D);
                 const int o = (pj + t) & 1;
                 const P2<T> xnext = take(sx1, fx, en);
@@ -458,9 +606,9 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const S
                 }
                 const T* C = cs0 + sc0 * CE;
                 const P2<T> b2 = sp_ld2<T>(C + OB + fc), cx2p = sp_ld2<TC>(C + OCX + fc);
-                const P2<T> cy2p = sp_ld2<TC>(C + OCY + fx), cyd2 = sp_ld2<TC>(C + OCY + fx - W);
+                const P2<T> cy2p = sp_ld2<TC>(C + OCY + fx), cyd2 = sp_ld2<TC>(C + cyd_off);
                 const P2<T> cz2 = sp_ld2<TC>(C + OCZ + fc);
-                const T cxl = (T)C[OCX + fc - 1];
+                const T cxl = (T)C[cxl_off];
                 T* X0 = xs0 + sx0 * XE;
                 if (role == 1 || o != side) { // a ring-column cell is relaxed where it is red
                     T xout = (T)0, xsv = (T)0, xnv = (T)0;
@@ -486,7 +634,7 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>()) sweep_pair_kernel(const S
                 advance();
             }
         }
-        asm volatile("cp.async.wait_all;" ::: "memory");
+        if constexpr (!TM) asm volatile("cp.async.wait_all;" ::: "memory");
     }
     if constexpr (DOT) {
         double v[1] = {dot_acc}, out[1];

@@ -169,7 +169,7 @@ static int sp_items_per_cta() {
     static int v = -1;
     if (v < 0) {
         const char* e = std::getenv("MF3D_SWEEP_ITEMS");
-        v = e ? std::max(1, std::atoi(e)) : 2;
+        v = e ? std::max(1, std::atoi(e)) : 1;
     }
     return v;
 }
@@ -183,23 +183,40 @@ static dim3 pair_grid(const Geom& g, long long resident, int* zchunk) {
     return dim3((unsigned)std::max(1LL, std::min(items, resident)));
 }
 
-template <class T, class TC>
-static void launch_pair_sweep(cudaStream_t s, dim3 grid, int mode, const SpArgs<T, TC>& a) {
-    const size_t smem = sp_smem_bytes<T, TC>();
+template <class T, class TC, bool TM>
+static void launch_pair_sweep_tm(cudaStream_t s, dim3 grid, int mode, const SpMaps& m, const SpArgs<T, TC>& a) {
+    const size_t smem = sp_smem_bytes<T, TC, TM>();
     switch (mode) {
-    case 0: sweep_pair_kernel<T, TC, 0><<<grid, SP_NT, smem, s>>>(a); break;
-    case M_ZERO: sweep_pair_kernel<T, TC, M_ZERO><<<grid, SP_NT, smem, s>>>(a); break;
-    case M_PROLONG: sweep_pair_kernel<T, TC, M_PROLONG><<<grid, SP_NT, smem, s>>>(a); break;
-    case M_ZERO | M_PROLONG: sweep_pair_kernel<T, TC, M_ZERO | M_PROLONG><<<grid, SP_NT, smem, s>>>(a); break;
-    case M_DOT: sweep_pair_kernel<T, TC, M_DOT><<<grid, SP_NT, smem, s>>>(a); break;
-    case M_ZERO | M_DOT: sweep_pair_kernel<T, TC, M_ZERO | M_DOT><<<grid, SP_NT, smem, s>>>(a); break;
-    case M_PROLONG | M_DOT: sweep_pair_kernel<T, TC, M_PROLONG | M_DOT><<<grid, SP_NT, smem, s>>>(a); break;
+    case 0: sweep_pair_kernel<T, TC, 0, TM><<<grid, SP_NT, smem, s>>>(m, a); break;
+    case M_ZERO: sweep_pair_kernel<T, TC, M_ZERO, TM><<<grid, SP_NT, smem, s>>>(m, a); break;
+    case M_PROLONG: sweep_pair_kernel<T, TC, M_PROLONG, TM><<<grid, SP_NT, smem, s>>>(m, a); break;
+    case M_ZERO | M_PROLONG: sweep_pair_kernel<T, TC, M_ZERO | M_PROLONG, TM><<<grid, SP_NT, smem, s>>>(m, a); break;
+    case M_DOT: sweep_pair_kernel<T, TC, M_DOT, TM><<<grid, SP_NT, smem, s>>>(m, a); break;
+    case M_ZERO | M_DOT: sweep_pair_kernel<T, TC, M_ZERO | M_DOT, TM><<<grid, SP_NT, smem, s>>>(m, a); break;
+    case M_PROLONG | M_DOT: sweep_pair_kernel<T, TC, M_PROLONG | M_DOT, TM><<<grid, SP_NT, smem, s>>>(m, a); break;
     case M_ZERO | M_PROLONG | M_DOT:
-        sweep_pair_kernel<T, TC, M_ZERO | M_PROLONG | M_DOT><<<grid, SP_NT, smem, s>>>(a);
+        sweep_pair_kernel<T, TC, M_ZERO | M_PROLONG | M_DOT, TM><<<grid, SP_NT, smem, s>>>(m, a);
         break;
     default: throw Error(MF3D_E_INVALID, "unsupported x-pair sweep mode");
     }
     MF3D_LAUNCH_CK();
+}
+template <class T, class TC>
+static void launch_pair_sweep(cudaStream_t s, dim3 grid, int mode, bool tm, const SpMaps& m, const SpArgs<T, TC>& a) {
+    if (tm) launch_pair_sweep_tm<T, TC, true>(s, grid, mode, m, a);
+    else launch_pair_sweep_tm<T, TC, false>(s, grid, mode, m, a);
+}
+// dynamic shared memory and resident CTAs per SM of one x-pair sweep variant
+template <class T, class TC, int MODE, bool TM> static int pair_sweep_setup() {
+    const size_t smem = sp_smem_bytes<T, TC, TM>();
+    MF3D_CK(cudaFuncSetAttribute(sweep_pair_kernel<T, TC, MODE, TM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    MF3D_CK(cudaFuncSetAttribute(sweep_pair_kernel<T, TC, MODE, TM>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared));
+    int n = 0;
+    MF3D_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_pair_kernel<T, TC, MODE, TM>, SP_NT, smem));
+    if (n < 1) throw Error(MF3D_E_CUDA, "x-pair sweep does not fit on an SM");
+    return n;
 }
 
 
@@ -373,6 +390,30 @@ template <class E> static CUtensorMap make_map2(const void* base, int d0, int d1
     return m;
 }
 
+// Whether the x-pair sweep stages a level by TMA: no periodic axis, and rows of the arrays
+// and of the boundary-face planes that are whole multiples of 16 bytes (a box row of
+// cp.async.bulk.tensor starts on a 16-byte boundary).
+template <class T> static bool sp_tma_ok(const Geom& g, const mf3d_bc& bc) {
+    if (bc.type[0] == MF3D_BC_PERIODIC || bc.type[2] == MF3D_BC_PERIODIC || bc.type[4] == MF3D_BC_PERIODIC)
+        return false;
+    return g.nx % 2 == 0 && ((size_t)g.nx * sizeof(T)) % 16 == 0 && ((size_t)g.ny * sizeof(T)) % 16 == 0;
+}
+// Tensor maps of the TMA-staged x-pair sweep of one level (x: the sweep's input buffer).
+template <class T, class TC>
+static SpMaps make_sp_maps(const Geom& g, const T* x, const T* b, const LevelOp<TC>& op) {
+    using G = SpGeom<T, true>;
+    SpMaps m;
+    m.x = make_map<T>(x, g, G::W, SP_XR);
+    m.b = make_map<T>(b, g, G::W, SP_CR);
+    m.cx = make_map<TC>(op.cx, g, G::W, SP_CR);
+    m.cy = make_map<TC>(op.cy, g, G::W, SP_YR);
+    m.cz = make_map<TC>(op.cz, g, G::W, SP_CR);
+    m.bxm = make_map2<TC>(op.bxm, g.ny, g.nz, G::BXN, 1);
+    m.bym = make_map2<TC>(op.bym, g.nx, g.nz, G::W, 1);
+    m.bzm = make_map2<TC>(op.bzm, g.nx, g.ny, G::W, SP_CR);
+    return m;
+}
+
 template <class T, class TC> class VCycle : public VCycleBase {
   public:
     // b0: level-0 right-hand side in the V-cycle's type (the PCG residual or its FP32 copy);
@@ -448,19 +489,28 @@ template <class T, class TC> class VCycle : public VCycleBase {
             }
         }
         if (n_tma_) set_tma_smem();
-        // levels the x-pair sweep serves (the FP64 V-cycle; single solves, every mode but the
-        // fused residual): nx even, periodic axes a whole number of tiles.  The FP32 V-cycle keeps
-        // the TMA quad sweep, measured faster in FP32 (0.152 against 0.203 ms for a plain sweep
-        // at 256^3), where it fits two CTAs per SM
+        // levels the x-pair sweep serves (single solves, every mode but the fused residual):
+        // the FP64 V-cycle wherever nx is even and a periodic axis is a whole number of tiles
+        // (TMA staging where the grid allows it, cp.async otherwise); the FP32 V-cycle where TMA
+        // staging applies (else the quad sweep); BF16 coefficients keep the quad sweep
         pair_.assign(Lt, 0);
-        if constexpr (sizeof(T) == 8 && sizeof(TC) == 8) {
+        pair_tm_.assign(Lt, 0);
+        pmaps_.resize(Lt);
+        if constexpr (sizeof(T) == sizeof(TC)) {
             for (int l = 0; l < Lt; ++l) {
                 const Geom& g = G[l];
                 if (g.nx % 2) continue;
                 if (bc.type[0] == MF3D_BC_PERIODIC && g.nx % SP_TX) continue;
                 if (bc.type[2] == MF3D_BC_PERIODIC && g.ny % SP_TY) continue;
+                if (sizeof(T) == 4 && !sp_tma_ok<T>(g, bc)) continue;
                 pair_[l] = 1;
                 ++n_pair_;
+                if (sp_tma_ok<T>(g, bc)) { // TMA staging; maps for both x buffers
+                    const T* b = l == 0 ? b0_ : (const T*)bl_[l]->p;
+                    pmaps_[l][0] = make_sp_maps<T, TC>(g, (const T*)xa_[l]->p, b, ops_[l]);
+                    pmaps_[l][1] = make_sp_maps<T, TC>(g, (const T*)xb_[l]->p, b, ops_[l]);
+                    pair_tm_[l] = 1;
+                }
             }
             if (n_pair_) set_pair_smem();
         }
@@ -820,15 +870,8 @@ template <class T, class TC> class VCycle : public VCycleBase {
     // ---- the x-pair sweep (kernels_sweep_pair.cuh) ----
     template <int MODE> void set_pair_one() {
         if constexpr (sizeof(T) == sizeof(TC)) {
-            const size_t smem = sp_smem_bytes<T, TC>();
-            MF3D_CK(cudaFuncSetAttribute(sweep_pair_kernel<T, TC, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem));
-            MF3D_CK(cudaFuncSetAttribute(sweep_pair_kernel<T, TC, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                         (int)cudaSharedmemCarveoutMaxShared));
-            int n = 0;
-            MF3D_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_pair_kernel<T, TC, MODE>, SP_NT, smem));
-            if (n < 1) throw Error(MF3D_E_CUDA, "x-pair sweep does not fit on an SM");
-            pocc_[MODE & 15] = n;
+            pocc_[MODE & 15] = pair_sweep_setup<T, TC, MODE, false>();
+            pocc_tm_[MODE & 15] = pair_sweep_setup<T, TC, MODE, true>();
         }
     }
     void set_pair_smem() {
@@ -858,10 +901,16 @@ template <class T, class TC> class VCycle : public VCycleBase {
             a.dot_partials = scr_.partials;
             a.dot_ticket = scr_.tickets + 0;
             a.dot_out = dot_out;
-            const long long resident = (long long)std::max(1, pocc_[mode & 15]) * num_sms();
+            a.err = scr_.err;
+            const bool tm = pair_tm_[l] != 0;
+            const long long resident = (long long)std::max(1, (tm ? pocc_tm_ : pocc_)[mode & 15]) * num_sms();
             const dim3 grid = pair_grid(g, resident, &a.zchunk);
             if ((mode & M_DOT) && grid.x > scr_.partial_cap) throw Error(MF3D_E_INVALID, "reduction scratch too small");
-            launch_pair_sweep<T, TC>(s, grid, mode, a);
+            static const SpMaps no_maps{};
+            const SpMaps& m = !tm ? no_maps : pmaps_[l][x_in == (const T*)xb_[l]->p ? 1 : 0];
+            if (tm && !(mode & M_ZERO) && x_in != (const T*)xa_[l]->p && x_in != (const T*)xb_[l]->p)
+                throw Error(MF3D_E_INVALID, "sweep input is not a level buffer");
+            launch_pair_sweep<T, TC>(s, grid, mode, tm, m, a);
         }
     }
 
@@ -958,9 +1007,11 @@ template <class T, class TC> class VCycle : public VCycleBase {
     // the fused sweep (cp.async moves at least 4 bytes).
     static constexpr bool split_resid_ = sizeof(TC) >= 4;
     int occ_[16] = {}; // resident staged-sweep CTAs per SM, by mode
-    std::vector<int> pair_; // levels served by the x-pair sweep
+    std::vector<int> pair_;    // levels served by the x-pair sweep
+    std::vector<int> pair_tm_; // ... with TMA staging
+    std::vector<std::array<SpMaps, 2>> pmaps_; // their tensor maps, x read from xa / xb
     int n_pair_ = 0;
-    int pocc_[16] = {}; // resident x-pair-sweep CTAs per SM, by mode
+    int pocc_[16] = {}, pocc_tm_[16] = {}; // resident x-pair-sweep CTAs per SM, by mode
     std::unique_ptr<DevMem> tail_out_, tail_w_;
     Tail2Args tail_{};
     size_t tail_smem_ = 0;
@@ -1854,24 +1905,30 @@ int mf3d_gsrb(const mf3d_grid* g, const mf3d_bc* bc, int pin, const double* K, c
         // the x-pair sweep where it applies (nx even, periodic axes whole tiles), as in the V-cycle
         if (g->nx % 2 == 0 && (bc->type[0] != MF3D_BC_PERIODIC || g->nx % SP_TX == 0) &&
             (bc->type[2] != MF3D_BC_PERIODIC || g->ny % SP_TY == 0)) {
-            const size_t smem = sp_smem_bytes<double, double>();
-            MF3D_CK(cudaFuncSetAttribute(sweep_pair_kernel<double, double, 0>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            int occ = 0;
-            MF3D_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sweep_pair_kernel<double, double, 0>, SP_NT, smem));
+            const bool tm = sp_tma_ok<double>(L.G, *bc);
+            const int occ = tm ? pair_sweep_setup<double, double, 0, true>() : pair_sweep_setup<double, double, 0, false>();
+            DevMem err(sizeof(int));
+            MF3D_CK(cudaMemsetAsync(err.p, 0, sizeof(int), s));
             SpArgs<double, double> a{};
             a.L = L.op;
             a.b = b;
+            a.err = err.as<int>();
             const dim3 grid = pair_grid(L.G, (long long)std::max(1, occ) * num_sms(), &a.zchunk);
+            SpMaps maps[2] = {};
+            if (tm)
+                for (int q = 0; q < 2; ++q) maps[q] = make_sp_maps<double, double>(L.G, pbufs[q], b, L.op);
             int cur = 0;
             for (int it = 0; it < iters; ++it) {
                 a.x_in = pbufs[cur];
                 a.x_out = pbufs[cur ^ 1];
-                launch_pair_sweep<double, double>(s, grid, 0, a);
+                launch_pair_sweep<double, double>(s, grid, 0, tm, maps[cur], a);
                 cur ^= 1;
             }
+            int e = 0;
+            MF3D_CK(cudaMemcpyAsync(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
             if (cur != 0) MF3D_CK(cudaMemcpyAsync(x, pbufs[cur], L.G.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
             MF3D_CK(cudaStreamSynchronize(s));
+            if (e) throw Error(MF3D_E_CUDA, "a TMA staging wait timed out in the smoother");
             return;
         }
         const int gx = (g->nx + SW_TX - 1) / SW_TX, gy = (g->ny + SW_TY - 1) / SW_TY;
