@@ -49,7 +49,7 @@
 
 namespace mf3d {
 
-constexpr int SP_TX = 32, SP_TY = 16; // tile (cells)
+constexpr int SP_TX = 32, SP_TY = 16; // tile of one x-pair per thread (cells); FP32 TMA tiles are 64 wide
 constexpr int SP_XR = SP_TY + 4;      // x rows j0-2 .. j0+TY+1
 constexpr int SP_CR = SP_TY + 2;      // b, cx, cz rows j0-1 .. j0+TY
 constexpr int SP_YR = SP_TY + 3;      // cy rows j0-2 .. j0+TY
@@ -65,8 +65,12 @@ constexpr int SP_NSC = SP_D;     // coefficient planes t .. t+D-1
 // box starts on a 16-byte boundary); every array of a slot starts on a 128-byte boundary.
 template <class T, bool TM> struct SpGeom {
     static constexpr int ST = (int)sizeof(T);
+    // x-pairs per thread: two (a quad of cells) in FP32 with TMA staging, where one pair per
+    // thread would move too few bytes per plane step; one otherwise
+    static constexpr int NP = (ST == 4 && TM) ? 2 : 1;
+    static constexpr int TX = SP_TX * NP; // tile width (cells)
     static constexpr int HX = TM ? 16 / ST : 2;
-    static constexpr int W = SP_TX + 2 * HX;
+    static constexpr int W = TX + 2 * HX;
     static constexpr int BXS = TM ? 16 / ST : 2; // the -x face buffer starts at row j0 - BXS
     static constexpr int BXN = SP_TY + 2 * BXS;
     static constexpr size_t a128(size_t v) { return (v + 127) & ~(size_t)127; }
@@ -80,8 +84,9 @@ template <class T, bool TM> struct SpGeom {
     static constexpr size_t SMEM = SP_NSX * XSB + SP_NSC * CSB + 128; // + alignment of the base
 };
 template <class T, class TC, bool TM> constexpr size_t sp_smem_bytes() { return SpGeom<T, TM>::SMEM; }
+template <class T, bool TM> constexpr int sp_tx() { return SpGeom<T, TM>::TX; }
 // resident CTAs per SM the register budget is cut for
-template <class T> constexpr int sp_minb() { return sizeof(T) == 8 ? 2 : 3; }
+template <class T, bool TM> constexpr int sp_minb() { return (sizeof(T) == 8 || SpGeom<T, TM>::NP == 2) ? 2 : 3; }
 
 template <class T, class TC> struct SpArgs {
     LevelOp<TC> L;
@@ -136,13 +141,13 @@ template <int B> __device__ __forceinline__ void sp_cp(uint32_t dst, const char*
 }
 
 template <class T, class TC, int MODE, bool TM>
-__global__ void __launch_bounds__(SP_NT, sp_minb<T>())
+__global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
     sweep_pair_kernel(const __grid_constant__ SpMaps maps, const SpArgs<T, TC> a) {
     static_assert(sizeof(T) == sizeof(TC) && sizeof(T) >= 4, "FP64 or FP32 vectors with coefficients of the same type");
     constexpr bool ZERO = (MODE & M_ZERO) != 0, PROL = (MODE & M_PROLONG) != 0, DOT = (MODE & M_DOT) != 0;
     static_assert((MODE & M_RESID) == 0, "the residual runs in a kernel of its own");
     using G = SpGeom<T, TM>;
-    constexpr int ST = G::ST, W = G::W, HX = G::HX;
+    constexpr int ST = G::ST, W = G::W, HX = G::HX, NP = G::NP, TX = G::TX;
     extern __shared__ __align__(128) unsigned char sp_sm_raw[];
     // slots start on a 128-byte boundary of the shared window (TMA destinations)
     unsigned char* const sp_sm =
@@ -160,7 +165,7 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>())
     const int nx = L.nx, ny = L.ny, nz = L.nz;
     const size_t nxy = (size_t)nx * ny;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int ntx = (nx + SP_TX - 1) / SP_TX, ntiles = ntx * ((ny + SP_TY - 1) / SP_TY);
+    const int ntx = (nx + TX - 1) / TX, ntiles = ntx * ((ny + SP_TY - 1) / SP_TY);
     const int total = ntiles * ((nz + a.zchunk - 1) / a.zchunk);
     const T dx2 = (T)L.dx2;
     auto divide = [](T num, T den) -> T {
@@ -190,7 +195,7 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>())
         __syncthreads(); // the previous item's reads (and generic writes) of the slots are done
         const int tile = item % ntiles;
         const int z0 = (item / ntiles) * a.zchunk, z1 = min(z0 + a.zchunk, nz);
-        const int i0 = (tile % ntx) * SP_TX, j0 = (tile / ntx) * SP_TY;
+        const int i0 = (tile % ntx) * TX, j0 = (tile / ntx) * SP_TY;
         const int P0 = z0 - 2;          // first x plane staged
         const int XL = z1 + 1, CL = z1; // last x plane, last coefficient plane
         // slots: x plane p in (p - P0) mod SP_NSX, coefficient plane q in (q - P0) mod SP_NSC.
@@ -371,22 +376,30 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>())
 
         if (role == 0) {
             // =============== tile pairs: red of plane t and black of plane t-1 ===============
-            const int pj = j0 + tyr, pi = i0 + 2 * lo;
-            const int wi = pi < nx ? pi : -1, wj = pj < ny ? pj : -1; // never wrapped
-            const bool pin_xy = wi >= 0 && wj >= 0;
-            const long long gxy = pin_xy ? (long long)wi + (long long)nx * wj : 0;
-            const int fx = (pj - j0 + 2) * W + (pi - i0 + HX), fc = fx - W;
-            // the -x face of cell pi - 1 and the -y faces of the pair: from the boundary-face
-            // buffers where the TMA form stages them, else from the cx / cy slots
-            const int cxl_off = (TM && i0 == 0 && pi == 0) ? OBX + (pj - j0 + G::BXS) : OCX + fc - 1;
-            const int cyd_off = (TM && j0 == 0 && pj == 0) ? OBY + (pi - i0 + HX) : OCY + fx - W;
+            // NP pairs per thread, side by side in one row: pair q starts at cell i0 + 2 (NP lo + q)
+            const int pj = j0 + tyr, pi0 = i0 + 2 * NP * lo;
+            const int wj = pj < ny ? pj : -1; // never wrapped
+            const int fx = (pj - j0 + 2) * W + (pi0 - i0 + HX), fc = fx - W;
+            bool pin[NP];
+            long long gxy[NP];
+            int cxl_off[NP], cyd_off[NP];
+#pragma unroll
+            for (int q = 0; q < NP; ++q) {
+                const int pi = pi0 + 2 * q;
+                pin[q] = pi < nx && wj >= 0;
+                gxy[q] = pin[q] ? (long long)pi + (long long)nx * wj : 0;
+                // the -x face of cell pi - 1 and the -y faces of the pair: from the boundary-face
+                // buffers where the TMA form stages them, else from the cx / cy slots
+                cxl_off[q] = (TM && i0 == 0 && pi == 0) ? OBX + (pj - j0 + G::BXS) : OCX + fc + 2 * q - 1;
+                cyd_off[q] = (TM && j0 == 0 && pj == 0) ? OBY + (pi - i0 + HX) : OCY + fx + 2 * q - W;
+            }
             auto issue = [&](int p) {
                 if constexpr (TM) {
                     tma_issue(p);
                 } else {
                     uint32_t xo, co;
                     slot_u(sxi, sci, xo, co);
-                    issue_pair(p, xo, co, pin_xy, gxy, wi, wj, fx, false, false, true, true);
+                    issue_pair(p, xo, co, pin[0], gxy[0], pi0, wj, fx, false, false, true, true);
                     asm volatile("cp.async.commit_group;" ::: "memory");
                 }
                 sxi = nxs(sxi);
@@ -400,90 +413,104 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>())
                 break;
             }
             const int wpar = warp & 1; // parity of this warp's rows (j0 is even)
-            const P2<T> xp0 = take(0, fx, corr(pin_xy, wi, wj, P0)); // x(P0): only its own column reads it
-            const P2<T> xp1 = take(1, fx, corr(pin_xy, wi, wj, P0 + 1)); // x(P0 + 1), published
-            T en = corr(pin_xy, wi, wj, P0 + 2); // correction of the pair in plane t + 1
-            P2<T> czp1 = sp_ld2<TC>(cs0 + OCZ + fc), czp2{(T)0, (T)0}; // cz of planes t-1, t-2
-            // carried: A = x(t).at(1-O), B = x(t-1).at(O), the red values of planes t-1 (column
-            // 1-O) and t-2 (column O), the black cell's coefficients of plane t-1 (column O)
             const int O0 = (wpar + z0 - 1) & 1;
-            T A = O0 ? xp1.a : xp1.b, B = O0 ? xp0.b : xp0.a;
-            T red1 = 0, red2 = 0, kb = 0, kxp = 0, kxm = 0, kyp = 0, kym = 0;
-            double2 r64n = make_double2(0.0, 0.0);
-            T* const xout_base = a.x_out + gxy;
+            // carried, per pair: A = x(t).at(1-O), B = x(t-1).at(O), the red values of planes t-1
+            // (column 1-O) and t-2 (column O), the black cell's coefficients of plane t-1
+            // (column O), cz of planes t-1 and t-2
+            T A[NP], B[NP], red1[NP], red2[NP], kb[NP], kxp[NP], kxm[NP], kyp[NP], kym[NP], en[NP];
+            P2<T> czp1[NP], czp2[NP];
+            double2 r64n[NP];
+#pragma unroll
+            for (int q = 0; q < NP; ++q) {
+                const int pi = pi0 + 2 * q;
+                const P2<T> xp0 = take(0, fx + 2 * q, corr(pin[q], pi, wj, P0)); // x(P0): own column only
+                const P2<T> xp1 = take(1, fx + 2 * q, corr(pin[q], pi, wj, P0 + 1)); // x(P0 + 1), published
+                en[q] = corr(pin[q], pi, wj, P0 + 2); // correction of the pair in plane t + 1
+                czp1[q] = sp_ld2<TC>(cs0 + OCZ + fc + 2 * q);
+                czp2[q] = P2<T>{(T)0, (T)0};
+                A[q] = O0 ? xp1.a : xp1.b;
+                B[q] = O0 ? xp0.b : xp0.a;
+                red1[q] = red2[q] = kb[q] = kxp[q] = kxm[q] = kyp[q] = kym[q] = (T)0;
+                r64n[q] = make_double2(0.0, 0.0);
+            }
 
             auto step = [&](auto Oc, int t) {
                 constexpr int O = decltype(Oc)::value;
                 issue(t + SP_D);
-                // ---- x of plane t+1 (own column; published for the neighbours with PROL) ----
-                T xnO;
-                if constexpr (PROL) {
-                    const P2<T> v = take(sx1, fx, en);
-                    xnO = O ? v.b : v.a;
-                    en = corr(pin_xy, wi, wj, t + 2);
-                } else if constexpr (ZERO) {
-                    xnO = (T)0;
-                } else {
-                    xnO = xs0[sx1 * XE + fx + O];
-                }
-                // ---- coefficients of plane t ----
                 const T* C = cs0 + sc0 * CE;
-                const P2<T> b2 = sp_ld2<T>(C + OB + fc), cx2p = sp_ld2<TC>(C + OCX + fc);
-                const P2<T> cy2p = sp_ld2<TC>(C + OCY + fx), cyd2 = sp_ld2<TC>(C + cyd_off);
-                const P2<T> cz2 = sp_ld2<TC>(C + OCZ + fc);
-                const T cxl = (T)C[cxl_off];
-                // ---- red cell pi + O of plane t, from old black values ----
                 T* X0 = xs0 + sx0 * XE;
-                T red = (T)0;
-                {
-                    T xout = (T)0, xsv = (T)0, xnv = (T)0;
-                    if constexpr (!ZERO || PROL) {
-                        xout = X0[fx - 1 + 3 * O];
-                        xsv = X0[fx - W + O];
-                        xnv = X0[fx + W + O];
+                const T* X1 = xs0 + sxm * XE;
+                const int q_out = t - 1;
+                const bool out_ok = q_out >= z0 && q_out < z1;
+#pragma unroll
+                for (int q = 0; q < NP; ++q) {
+                    const int f = fx + 2 * q, g = fc + 2 * q;
+                    // ---- x of plane t+1 (own column; published for the neighbours with PROL) ----
+                    T xnO;
+                    if constexpr (PROL) {
+                        const P2<T> v = take(sx1, f, en[q]);
+                        xnO = O ? v.b : v.a;
+                        en[q] = corr(pin[q], pi0 + 2 * q, wj, t + 2);
+                    } else if constexpr (ZERO) {
+                        xnO = (T)0;
+                    } else {
+                        xnO = xs0[sx1 * XE + f + O];
                     }
-                    const T xw = O ? A : xout, xe = O ? xout : A;
-                    const T cxp = O ? cx2p.b : cx2p.a, cxm = O ? cx2p.a : cxl;
-                    const T cyp = O ? cy2p.b : cy2p.a, cym = O ? cyd2.b : cyd2.a;
-                    const T czp = O ? cz2.b : cz2.a, czm = O ? czp1.b : czp1.a;
-                    T D = cxm + cxp + cym + cyp + czm + czp;
-                    if (O == 0 && L.pin && pi == 0 && pj == 0 && zzero(t)) D *= (T)2; // cell 0 is red
-                    const T sum = cxp * xe + cxm * xw + cyp * xnv + cym * xsv + czp * xnO + czm * B;
-                    const T bb = O ? b2.b : b2.a;
-                    if (pin_xy && zin(t)) red = divide(sum - bb * dx2, D);
+                    // ---- coefficients of plane t ----
+                    const P2<T> b2 = sp_ld2<T>(C + OB + g), cx2p = sp_ld2<TC>(C + OCX + g);
+                    const P2<T> cy2p = sp_ld2<TC>(C + OCY + f), cyd2 = sp_ld2<TC>(C + cyd_off[q]);
+                    const P2<T> cz2 = sp_ld2<TC>(C + OCZ + g);
+                    const T cxl = (T)C[cxl_off[q]];
+                    // ---- red cell pi + O of plane t, from old black values ----
+                    T red = (T)0;
+                    {
+                        T xout = (T)0, xsv = (T)0, xnv = (T)0;
+                        if constexpr (!ZERO || PROL) {
+                            xout = X0[f - 1 + 3 * O];
+                            xsv = X0[f - W + O];
+                            xnv = X0[f + W + O];
+                        }
+                        const T xw = O ? A[q] : xout, xe = O ? xout : A[q];
+                        const T cxp = O ? cx2p.b : cx2p.a, cxm = O ? cx2p.a : cxl;
+                        const T cyp = O ? cy2p.b : cy2p.a, cym = O ? cyd2.b : cyd2.a;
+                        const T czp = O ? cz2.b : cz2.a, czm = O ? czp1[q].b : czp1[q].a;
+                        T D = cxm + cxp + cym + cyp + czm + czp;
+                        if (O == 0 && L.pin && pi0 + 2 * q == 0 && pj == 0 && zzero(t)) D *= (T)2; // cell 0 is red
+                        const T sum = cxp * xe + cxm * xw + cyp * xnv + cym * xsv + czp * xnO + czm * B[q];
+                        const T bb = O ? b2.b : b2.a;
+                        if (pin[q] && zin(t)) red = divide(sum - bb * dx2, D);
+                    }
+                    X0[f + O] = red;
+                    // ---- black cell pi + O of plane t-1 from red values; plane t-1 is then final ----
+                    if (out_ok && pin[q]) {
+                        const T xout = X1[f - 1 + 3 * O], xsv = X1[f - W + O], xnv = X1[f + W + O];
+                        const T xw = O ? red1[q] : xout, xe = O ? xout : red1[q];
+                        const T kzp = O ? czp1[q].b : czp1[q].a, kzm = O ? czp2[q].b : czp2[q].a;
+                        const T D = kxm[q] + kxp[q] + kym[q] + kyp[q] + kzm + kzp;
+                        const T sum = kxp[q] * xe + kxm[q] * xw + kyp[q] * xnv + kym[q] * xsv + kzp * red + kzm * red2[q];
+                        const T blk = divide(sum - kb[q] * dx2, D);
+                        const T va = O ? red1[q] : blk, vb = O ? blk : red1[q];
+                        sp_stg2<T>(a.x_out + (size_t)gxy[q] + nxy * (size_t)q_out, va, vb);
+                        if constexpr (DOT) dot_acc += r64n[q].x * (double)va + r64n[q].y * (double)vb;
+                    }
+                    if constexpr (DOT) { // r64 of plane t, for the output of plane t at the next step
+                        const bool out_t = t >= z0 && t < z1 && pin[q];
+                        r64n[q] = out_t ? __ldg(reinterpret_cast<const double2*>(a.r64 + (size_t)gxy[q] + nxy * (size_t)t))
+                                        : make_double2(0.0, 0.0);
+                    }
+                    // ---- carry to the next plane (red offset 1 - O) ----
+                    B[q] = A[q];
+                    A[q] = xnO;
+                    red2[q] = red1[q];
+                    red1[q] = red;
+                    kb[q] = O ? b2.a : b2.b;
+                    kxp[q] = O ? cx2p.a : cx2p.b;
+                    kxm[q] = O ? cxl : cx2p.a;
+                    kyp[q] = O ? cy2p.a : cy2p.b;
+                    kym[q] = O ? cyd2.a : cyd2.b;
+                    czp2[q] = czp1[q];
+                    czp1[q] = cz2;
                 }
-                X0[fx + O] = red;
-                // ---- black cell pi + O of plane t-1 from red values; plane t-1 is then final ----
-                const int q = t - 1;
-                if (q >= z0 && q < z1 && pin_xy) {
-                    const T* X1 = xs0 + sxm * XE;
-                    const T xout = X1[fx - 1 + 3 * O], xsv = X1[fx - W + O], xnv = X1[fx + W + O];
-                    const T xw = O ? red1 : xout, xe = O ? xout : red1;
-                    const T kzp = O ? czp1.b : czp1.a, kzm = O ? czp2.b : czp2.a;
-                    const T D = kxm + kxp + kym + kyp + kzm + kzp;
-                    const T sum = kxp * xe + kxm * xw + kyp * xnv + kym * xsv + kzp * red + kzm * red2;
-                    const T blk = divide(sum - kb * dx2, D);
-                    const T va = O ? red1 : blk, vb = O ? blk : red1;
-                    sp_stg2<T>(xout_base + nxy * (size_t)q, va, vb);
-                    if constexpr (DOT) dot_acc += r64n.x * (double)va + r64n.y * (double)vb;
-                }
-                if constexpr (DOT) { // r64 of plane t, for the output of plane t at the next step
-                    const bool out_t = t >= z0 && t < z1 && pin_xy;
-                    r64n = out_t ? __ldg(reinterpret_cast<const double2*>(a.r64 + (size_t)gxy + nxy * (size_t)t))
-                                 : make_double2(0.0, 0.0);
-                }
-                // ---- carry to the next plane (red offset 1 - O) ----
-                B = A;
-                A = xnO;
-                red2 = red1;
-                red1 = red;
-                kb = O ? b2.a : b2.b;
-                kxp = O ? cx2p.a : cx2p.b;
-                kxm = O ? cxl : cx2p.a;
-                kyp = O ? cy2p.a : cy2p.b;
-                kym = O ? cyd2.a : cyd2.b;
-                czp2 = czp1;
-                czp1 = cz2;
             };
             using Z = std::integral_constant<int, 0>;
             using I = std::integral_constant<int, 1>;
@@ -502,82 +529,90 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>())
             }
         } else {
             // =============== ring pairs / cells: red of plane t only ===============
-            int pj, pi, side = -1;
-            if (role == 1) pj = hi ? j0 + SP_TY : j0 - 1, pi = i0 + 2 * lo;
-            else side = hi, pj = j0 + lo, pi = hi ? i0 + SP_TX : i0 - 2;
-            const int wi = wrap_or_out(pi, nx, L.per_x), wj = wrap_or_out(pj, ny, L.per_y);
-            const bool pin_xy = wi >= 0 && wj >= 0;
-            const long long gxy = pin_xy ? (long long)wi + (long long)nx * wj : 0;
-            const int fx = (pj - j0 + 2) * W + (pi - i0 + HX), fc = fx - W;
-            const int cxl_off = (TM && i0 == 0 && pi == 0) ? OBX + (pj - j0 + G::BXS) : OCX + fc - 1;
-            const int cyd_off = (TM && j0 == 0 && pj == 0) ? OBY + (pi - i0 + HX) : OCY + fx - W;
-            // second x pair: the ring-row warp the outer rows, ring-column lanes 0/1 of each side
-            // the corner pairs (rows j0-1, j0+TY)
+            // ring-row lanes: NP pairs side by side; ring-column lanes: one cell (its side pair)
+            int pj, pi0, side = -1;
+            if (role == 1) pj = hi ? j0 + SP_TY : j0 - 1, pi0 = i0 + 2 * NP * lo;
+            else side = hi, pj = j0 + lo, pi0 = hi ? i0 + TX : i0 - 2;
+            const int npair = role == 1 ? NP : 1;
+            const int wj = wrap_or_out(pj, ny, L.per_y);
+            const int fx = (pj - j0 + 2) * W + (pi0 - i0 + HX), fc = fx - W;
+            // second x pair(s): the ring-row warp the outer rows, ring-column lanes 0/1 of each
+            // side the corner pairs (rows j0-1, j0+TY)
             int sj = 0;
             bool has2 = false;
             if (role == 1) has2 = true, sj = hi ? j0 + SP_TY + 1 : j0 - 2;
             else if (lo == 0 || lo == 1) has2 = true, sj = lo ? j0 + SP_TY : j0 - 1;
             const int wj2 = wrap_or_out(sj, ny, L.per_y);
-            const bool pin2 = has2 && wi >= 0 && wj2 >= 0;
-            const long long gxy2 = pin2 ? (long long)wi + (long long)nx * wj2 : 0;
-            const int fx2 = (sj - j0 + 2) * W + (pi - i0 + HX);
-            // coefficients beyond the pair's own: cx of the left corner pairs (ring-column lanes
-            // 0 / 1 of the left side: the -x faces of the ring-row cells at i0), cy of the row
-            // below the ring row (ring-row lanes 0-15) and of row j0-1 beside the tile
-            // (ring-column lanes 0 / 16: the -y faces of the ring-column cells at j0)
+            const int fx2 = (sj - j0 + 2) * W + (pi0 - i0 + HX);
+            // coefficients beyond the pair's own (cp.async form): cx of the left corner pairs
+            // (ring-column lanes 0 / 1 of the left side: the -x faces of the ring-row cells at
+            // i0), cy of the row below the ring row (ring-row lanes 0-15) and of row j0-1 beside
+            // the tile (ring-column lanes 0 / 16: the -y faces of the ring-column cells at j0)
             const bool cx2 = role == 2 && side == 0 && has2;
             const bool cy2 = (role == 1 && !hi) || (role == 2 && lo == 0);
             const int cy2j = role == 1 ? j0 - 2 : j0 - 1;
             const int wcy2 = wrap_or_out(cy2j, ny, L.per_y);
-            const bool cx_bnd = pi == -2 && !L.per_x, cy_bnd = pj == -1 && !L.per_y;
+            const bool cy_bnd = pj == -1 && !L.per_y;
             const bool cy2_bnd = cy2j == -1 && !L.per_y;
-            const long long gcy2 = (wi >= 0 && wcy2 >= 0) ? (long long)wi + (long long)nx * wcy2 : 0;
-            const int fyy = (cy2j - j0 + 2) * W + (pi - i0 + HX);
+            const int fyy = (cy2j - j0 + 2) * W + (pi0 - i0 + HX);
+            int wi[NP], cxl_off[NP], cyd_off[NP];
+            bool pin[NP], pin2[NP], cx_bnd[NP];
+            long long gxy[NP], gxy2[NP], gcy2[NP];
+#pragma unroll
+            for (int q = 0; q < NP; ++q) {
+                const int pi = pi0 + 2 * q;
+                wi[q] = wrap_or_out(pi, nx, L.per_x);
+                pin[q] = q < npair && wi[q] >= 0 && wj >= 0;
+                gxy[q] = pin[q] ? (long long)wi[q] + (long long)nx * wj : 0;
+                pin2[q] = q < npair && has2 && wi[q] >= 0 && wj2 >= 0;
+                gxy2[q] = pin2[q] ? (long long)wi[q] + (long long)nx * wj2 : 0;
+                gcy2[q] = (wi[q] >= 0 && wcy2 >= 0) ? (long long)wi[q] + (long long)nx * wcy2 : 0;
+                cx_bnd[q] = pi == -2 && !L.per_x;
+                cxl_off[q] = (TM && i0 == 0 && pi == 0) ? OBX + (pj - j0 + G::BXS) : OCX + fc + 2 * q - 1;
+                cyd_off[q] = (TM && j0 == 0 && pj == 0) ? OBY + (pi - i0 + HX) : OCY + fx + 2 * q - W;
+            }
             auto issue = [&](int p) {
-                if constexpr (TM) { // thread 0 stages everything
-                    sxi = nxs(sxi);
-                    sci = ncs(sci);
-                    return;
-                }
-                uint32_t xo, co;
-                slot_u(sxi, sci, xo, co);
-                issue_pair(p, xo, co, pin_xy, gxy, wi, wj, fx, cx_bnd, cy_bnd, true, true);
-                if (has2) { // x of the second pair; cx of a corner pair
-                    issue_pair(p, xo, co, pin2, gxy2, wi, wj2, fx2, false, false, true, false);
-                    if (cx2) { // only cx of plane p - 1 (b, cy, cz of the corner are not read)
+                if constexpr (!TM) { // (one pair per lane: NP == 1 in this form)
+                    uint32_t xo, co;
+                    slot_u(sxi, sci, xo, co);
+                    issue_pair(p, xo, co, pin[0], gxy[0], wi[0], wj, fx, cx_bnd[0], cy_bnd, true, true);
+                    if (has2) { // x of the second pair; cx of a corner pair
+                        issue_pair(p, xo, co, pin2[0], gxy2[0], wi[0], wj2, fx2, false, false, true, false);
+                        if (cx2) { // only cx of plane p - 1 (b, cy, cz of the corner are not read)
+                            const int q = p - 1;
+                            if (q >= P0 && q <= CL) {
+                                T* Cb = reinterpret_cast<T*>(sp_sm + (co - xs0_u));
+                                const int kz = wrap_or_out(q, nz, L.per_z);
+                                const bool kin = kz >= 0;
+                                if (cx_bnd[0]) {
+                                    const bool okb = wj2 >= 0 && kin;
+                                    pmv_cp<ST>(Cb + OCX + fx2 - W + 1, L.bxm + (okb ? (size_t)wj2 + (size_t)ny * kz : 0), okb);
+                                } else {
+                                    const bool ok2 = pin2[0] && kin;
+                                    pmv_cp<2 * ST>(Cb + OCX + fx2 - W,
+                                                   L.cx + (ok2 ? (size_t)gxy2[0] + nxy * (size_t)kz : 0), ok2);
+                                }
+                            }
+                        }
+                    }
+                    if (cy2) { // cy of plane p - 1 in row cy2j
                         const int q = p - 1;
                         if (q >= P0 && q <= CL) {
                             T* Cb = reinterpret_cast<T*>(sp_sm + (co - xs0_u));
                             const int kz = wrap_or_out(q, nz, L.per_z);
                             const bool kin = kz >= 0;
-                            if (cx_bnd) {
-                                const bool okb = wj2 >= 0 && kin;
-                                pmv_cp<ST>(Cb + OCX + fx2 - W + 1, L.bxm + (okb ? (size_t)wj2 + (size_t)ny * kz : 0), okb);
+                            if (cy2_bnd) {
+                                const bool okb = wi[0] >= 0 && kin;
+                                pmv_cp<2 * ST>(Cb + OCY + fyy, L.bym + (okb ? (size_t)wi[0] + (size_t)nx * kz : 0), okb);
                             } else {
-                                const bool ok2 = pin2 && kin;
-                                pmv_cp<2 * ST>(Cb + OCX + fx2 - W,
-                                               L.cx + (ok2 ? (size_t)gxy2 + nxy * (size_t)kz : 0), ok2);
+                                const bool ok2 = wi[0] >= 0 && wcy2 >= 0 && kin;
+                                pmv_cp<2 * ST>(Cb + OCY + fyy, L.cy + (ok2 ? (size_t)gcy2[0] + nxy * (size_t)kz : 0), ok2);
                             }
                         }
                     }
+                    asm volatile("cp.async.commit_group;" ::: "memory");
                 }
-                if (cy2) { // cy of plane p - 1 in row cy2j
-                    const int q = p - 1;
-                    if (q >= P0 && q <= CL) {
-                        T* Cb = reinterpret_cast<T*>(sp_sm + (co - xs0_u));
-                        const int kz = wrap_or_out(q, nz, L.per_z);
-                        const bool kin = kz >= 0;
-                        if (cy2_bnd) {
-                            const bool okb = wi >= 0 && kin;
-                            pmv_cp<2 * ST>(Cb + OCY + fyy, L.bym + (okb ? (size_t)wi + (size_t)nx * kz : 0), okb);
-                        } else {
-                            const bool ok2 = wi >= 0 && wcy2 >= 0 && kin;
-                            pmv_cp<2 * ST>(Cb + OCY + fyy, L.cy + (ok2 ? (size_t)gcy2 + nxy * (size_t)kz : 0), ok2);
-                        }
-                    }
-                }
-                asm volatile("cp.async.commit_group;" ::: "memory");
-                sxi = nxs(sxi);
+                sxi = nxs(sxi); // (TMA form: thread 0 stages everything)
                 sci = ncs(sci);
             };
 #pragma unroll
@@ -586,11 +621,22 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>())
                 fail = true;
                 break;
             }
-            P2<T> xprev = take(0, fx, corr(pin_xy, wi, wj, P0));
-            P2<T> xcur = take(1, fx, corr(pin_xy, wi, wj, P0 + 1));
-            if (has2) (void)take(1, fx2, corr(pin2, wi, wj2, P0 + 1));
-            T en = corr(pin_xy, wi, wj, P0 + 2), en2 = has2 ? corr(pin2, wi, wj2, P0 + 2) : (T)0;
-            P2<T> czp1 = sp_ld2<TC>(cs0 + OCZ + fc);
+            P2<T> xprev[NP], xcur[NP], czp1[NP];
+            T en[NP], en2[NP];
+#pragma unroll
+            for (int q = 0; q < NP; ++q) {
+                // (a ring-column lane has one pair: its slot neighbour belongs to the tile, and the
+                // correction written back by take() must not touch it)
+                xprev[q] = xcur[q] = czp1[q] = P2<T>{(T)0, (T)0};
+                en[q] = en2[q] = (T)0;
+                if (q >= npair) continue;
+                xprev[q] = take(0, fx + 2 * q, corr(pin[q], wi[q], wj, P0));
+                xcur[q] = take(1, fx + 2 * q, corr(pin[q], wi[q], wj, P0 + 1));
+                if (has2) (void)take(1, fx2 + 2 * q, corr(pin2[q], wi[q], wj2, P0 + 1));
+                en[q] = corr(pin[q], wi[q], wj, P0 + 2);
+                en2[q] = has2 ? corr(pin2[q], wi[q], wj2, P0 + 2) : (T)0;
+                czp1[q] = sp_ld2<TC>(cs0 + OCZ + fc + 2 * q);
+            }
             for (int t = z0 - 1; t <= z1; ++t) {
                 if (!sync_step(t + 1, sx1)) {
                     fail = true;
@@ -598,39 +644,45 @@ __global__ void __launch_bounds__(SP_NT, sp_minb<T>())
                 }
                 issue(t + SP_D);
                 const int o = (pj + t) & 1;
-                const P2<T> xnext = take(sx1, fx, en);
-                if (has2) (void)take(sx1, fx2, en2);
-                if constexpr (PROL) {
-                    en = corr(pin_xy, wi, wj, t + 2);
-                    if (has2) en2 = corr(pin2, wi, wj2, t + 2);
-                }
                 const T* C = cs0 + sc0 * CE;
-                const P2<T> b2 = sp_ld2<T>(C + OB + fc), cx2p = sp_ld2<TC>(C + OCX + fc);
-                const P2<T> cy2p = sp_ld2<TC>(C + OCY + fx), cyd2 = sp_ld2<TC>(C + cyd_off);
-                const P2<T> cz2 = sp_ld2<TC>(C + OCZ + fc);
-                const T cxl = (T)C[cxl_off];
                 T* X0 = xs0 + sx0 * XE;
-                if (role == 1 || o != side) { // a ring-column cell is relaxed where it is red
-                    T xout = (T)0, xsv = (T)0, xnv = (T)0;
-                    if constexpr (!ZERO || PROL) {
-                        xout = X0[fx - 1 + 3 * o];
-                        xsv = X0[fx - W + o];
-                        xnv = X0[fx + W + o];
+#pragma unroll
+                for (int q = 0; q < NP; ++q) {
+                    if (q >= npair) break;
+                    const int f = fx + 2 * q, g = fc + 2 * q;
+                    const P2<T> xnext = take(sx1, f, en[q]);
+                    if (has2) (void)take(sx1, fx2 + 2 * q, en2[q]);
+                    if constexpr (PROL) {
+                        en[q] = corr(pin[q], wi[q], wj, t + 2);
+                        if (has2) en2[q] = corr(pin2[q], wi[q], wj2, t + 2);
                     }
-                    const T xin = xcur.at(1 - o);
-                    const T xw = o ? xin : xout, xe = o ? xout : xin;
-                    const T cxp = cx2p.at(o), cxm = o ? cx2p.a : cxl;
-                    const T cyp = cy2p.at(o), cym = cyd2.at(o), czp = cz2.at(o), czm = czp1.at(o);
-                    T D = cxm + cxp + cym + cyp + czm + czp;
-                    if (L.pin && wi == 0 && wj == 0 && o == 0 && zzero(t)) D *= (T)2;
-                    const T sum = cxp * xe + cxm * xw + cyp * xnv + cym * xsv + czp * xnext.at(o) + czm * xprev.at(o);
-                    T red = (T)0;
-                    if (pin_xy && zin(t)) red = divide(sum - b2.at(o) * dx2, D);
-                    X0[fx + o] = red;
+                    const P2<T> b2 = sp_ld2<T>(C + OB + g), cx2p = sp_ld2<TC>(C + OCX + g);
+                    const P2<T> cy2p = sp_ld2<TC>(C + OCY + f), cyd2 = sp_ld2<TC>(C + cyd_off[q]);
+                    const P2<T> cz2 = sp_ld2<TC>(C + OCZ + g);
+                    const T cxl = (T)C[cxl_off[q]];
+                    if (role == 1 || o != side) { // a ring-column cell is relaxed where it is red
+                        T xout = (T)0, xsv = (T)0, xnv = (T)0;
+                        if constexpr (!ZERO || PROL) {
+                            xout = X0[f - 1 + 3 * o];
+                            xsv = X0[f - W + o];
+                            xnv = X0[f + W + o];
+                        }
+                        const T xin = xcur[q].at(1 - o);
+                        const T xw = o ? xin : xout, xe = o ? xout : xin;
+                        const T cxp = cx2p.at(o), cxm = o ? cx2p.a : cxl;
+                        const T cyp = cy2p.at(o), cym = cyd2.at(o), czp = cz2.at(o), czm = czp1[q].at(o);
+                        T D = cxm + cxp + cym + cyp + czm + czp;
+                        if (L.pin && wi[q] == 0 && wj == 0 && o == 0 && zzero(t)) D *= (T)2;
+                        const T sum = cxp * xe + cxm * xw + cyp * xnv + cym * xsv + czp * xnext.at(o) +
+                                      czm * xprev[q].at(o);
+                        T red = (T)0;
+                        if (pin[q] && zin(t)) red = divide(sum - b2.at(o) * dx2, D);
+                        X0[f + o] = red;
+                    }
+                    xprev[q] = xcur[q];
+                    xcur[q] = xnext;
+                    czp1[q] = cz2;
                 }
-                xprev = xcur;
-                xcur = xnext;
-                czp1 = cz2;
                 advance();
             }
         }

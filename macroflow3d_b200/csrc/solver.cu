@@ -173,8 +173,8 @@ static int sp_items_per_cta() {
     }
     return v;
 }
-static dim3 pair_grid(const Geom& g, long long resident, int* zchunk) {
-    const long long tiles = (long long)((g.nx + SP_TX - 1) / SP_TX) * ((g.ny + SP_TY - 1) / SP_TY);
+static dim3 pair_grid(const Geom& g, long long resident, int* zchunk, int tx = SP_TX) {
+    const long long tiles = (long long)((g.nx + tx - 1) / tx) * ((g.ny + SP_TY - 1) / SP_TY);
     const long long want = resident * sp_items_per_cta();
     const long long nchunk = std::max<long long>(1, std::min<long long>(g.nz, want / std::max(1LL, tiles)));
     const int zc = (int)((g.nz + nchunk - 1) / nchunk);
@@ -904,7 +904,7 @@ template <class T, class TC> class VCycle : public VCycleBase {
             a.err = scr_.err;
             const bool tm = pair_tm_[l] != 0;
             const long long resident = (long long)std::max(1, (tm ? pocc_tm_ : pocc_)[mode & 15]) * num_sms();
-            const dim3 grid = pair_grid(g, resident, &a.zchunk);
+            const dim3 grid = pair_grid(g, resident, &a.zchunk, tm ? sp_tx<T, true>() : sp_tx<T, false>());
             if ((mode & M_DOT) && grid.x > scr_.partial_cap) throw Error(MF3D_E_INVALID, "reduction scratch too small");
             static const SpMaps no_maps{};
             const SpMaps& m = !tm ? no_maps : pmaps_[l][x_in == (const T*)xb_[l]->p ? 1 : 0];
@@ -1913,7 +1913,8 @@ int mf3d_gsrb(const mf3d_grid* g, const mf3d_bc* bc, int pin, const double* K, c
             a.L = L.op;
             a.b = b;
             a.err = err.as<int>();
-            const dim3 grid = pair_grid(L.G, (long long)std::max(1, occ) * num_sms(), &a.zchunk);
+            const dim3 grid = pair_grid(L.G, (long long)std::max(1, occ) * num_sms(), &a.zchunk,
+                                        tm ? sp_tx<double, true>() : sp_tx<double, false>());
             SpMaps maps[2] = {};
             if (tm)
                 for (int q = 0; q < 2; ++q) maps[q] = make_sp_maps<double, double>(L.G, pbufs[q], b, L.op);

@@ -15,12 +15,17 @@ pytestmark = pytest.mark.gpu
 # both arms stop at ||r||/||b|| <= 1e-10; their iterates differ by rounding only
 HEAD_TOL = 1e-8
 # after a fixed number of iterations the iterates agree to rounding (the batch sums the
-# in-sweep <r, z> per work item, the single solve per CTA)
-ITERATE_TOL = 1e-10
+# in-sweep <r, z> per work item, the single solve per CTA).  In FP32 the single solve smooths
+# with the x-pair sweep and the batch with the quad sweep, two kernels that round differently
+# in FP32 (measured up to 2.4e-6 after six iterations on these grids); in FP64 both agree to
+# 1e-14.  Converged heads are compared at HEAD_TOL, and with the oracle in test_batch_vs_oracle
+ITERATE_TOL = {"fp32": 1e-4, "fp64": 1e-10}
 # ||r|| after six iterations (1e-5 of ||r0||) relative to each other: a single solve takes
-# the residual of the last pre-sweep in a kernel of its own, the batch inside the fused sweep,
-# and in FP32 the two round differently
-RESID_TOL = {"fp32": 1e-5, "fp64": 1e-6}
+# the residual of the last pre-sweep in a kernel of its own, the batch inside the fused sweep;
+# in FP32 the two sweep kernels also round differently, and a 1e-7 difference in the V-cycle's
+# output becomes several per cent of a residual six digits below ||r0|| (measured up to 6%):
+# FP32 only asks for the same convergence rate (within a factor 1.5)
+RESID_TOL = {"fp32": 0.5, "fp64": 1e-6}
 # near the stopping threshold the plain FP64 method (Fletcher-Reeves beta with the reference's
 # non-symmetric V-cycle) converges unevenly, so a rounding difference can move the stop by an
 # iteration or two; the flexible mixed-precision method does not
@@ -105,8 +110,8 @@ def test_batch_iterates_match_single_solves(mf3d, prec):
     b, got, _ = _batch(M, grids, bc, cfg, Ks)
     for (hr, rr), (hb, rb) in zip(ref, got):
         assert rr.num_iterations == rb.num_iterations == 6 and not rb.converged
-        assert _rel(hb, hr) < ITERATE_TOL
-        assert abs(rb.final_residual - rr.final_residual) <= RESID_TOL[prec] * rr.final_residual
+        assert _rel(hb, hr) < ITERATE_TOL[prec]
+        assert abs(rb.final_residual - rr.final_residual) <= RESID_TOL[prec] * rr.final_residual, prec
     b.close()
 
 
