@@ -2,6 +2,8 @@
 //
 // One kernel writes all three components (the reference launches 3 interior + 6 boundary
 // kernels on the legacy default stream, src/physics/flow/velocity_from_head.cu:601-777).
+// Each cell writes its three min-side faces; the plus faces are evaluated only at the max
+// boundary, or for the mass balance, so an interior face is computed once.
 // Formulas are the reference's: interior q = -[2 K_L K_R / (K_L + K_R)] (h_R - h_L)/dx;
 // Dirichlet faces -K_c (h_c - h_bc)/(dx/2) (min side) and -K_c (h_bc - h_c)/(dx/2) (max side);
 // Neumann 0; periodic faces use the wrapped neighbour (velocity_from_head.cu:102-381).
@@ -11,7 +13,11 @@
 
 namespace mf3d {
 
-__device__ __forceinline__ double hm_vel(double a, double b) { return 2.0 * a * b / (a + b); }
+// Flux through an interior (or periodic) face from cell L to cell R: -[2 K_L K_R / (K_L + K_R)]
+// (h_R - h_L) / d, evaluated with one division (the reference's two differ in rounding only).
+__device__ __forceinline__ double flux_lr(double KL, double KR, double HL, double HR, double d) {
+    return (2.0 * KL * KR * (HL - HR)) / ((KL + KR) * d);
+}
 
 struct VelOut {
     double* U;
@@ -38,15 +44,15 @@ __device__ __forceinline__ size_t w_idx(int layout, int i, int j, int k, int nx,
 // in-domain neighbour otherwise.
 __device__ __forceinline__ double face_min(const double* H, const double* K, size_t c, size_t cn, size_t cw,
                                            bool lo, int type, double hbc, double d) {
-    if (!lo) return -hm_vel(K[cn], K[c]) * (H[c] - H[cn]) / d;
+    if (!lo) return flux_lr(K[cn], K[c], H[cn], H[c], d);
     if (type == BC_DIRICHLET) return -K[c] * (H[c] - hbc) / (d * 0.5);
-    if (type == BC_PERIODIC) return -hm_vel(K[cw], K[c]) * (H[c] - H[cw]) / d;
+    if (type == BC_PERIODIC) return flux_lr(K[cw], K[c], H[cw], H[c], d);
     return 0.0;
 }
 __device__ __forceinline__ double face_max_bnd(const double* H, const double* K, size_t c, size_t cw, int type,
                                                double hbc, double d) {
     if (type == BC_DIRICHLET) return -K[c] * (hbc - H[c]) / (d * 0.5);
-    if (type == BC_PERIODIC) return -hm_vel(K[c], K[cw]) * (H[cw] - H[c]) / d;
+    if (type == BC_PERIODIC) return flux_lr(K[c], K[cw], H[c], H[cw], d);
     return 0.0;
 }
 
@@ -72,22 +78,26 @@ __global__ void __launch_bounds__(VEL_NT) velocity_kernel(int nx, int ny, int nz
         o.U[u_idx(o.layout, i, j, k, nx, ny)] = u0;
         o.V[v_idx(o.layout, i, j, k, nx, ny)] = v0;
         o.W[w_idx(o.layout, i, j, k, nx, ny)] = w0;
-        // plus faces: the neighbour's min face, or the max boundary
-        double u1, v1, w1;
-        if (i < nx - 1) u1 = -hm_vel(K[c], K[c + 1]) * (H[c + 1] - H[c]) / dx;
-        else {
+        // plus faces: at the max boundary (written here), and for the mass balance the
+        // neighbour's min face, with the same arithmetic as that neighbour's store
+        double u1 = 0.0, v1 = 0.0, w1 = 0.0;
+        if (i == nx - 1) {
             u1 = face_max_bnd(H, K, c, c - (nx - 1), bc.type[1], bc.value[1], dx);
             o.U[u_idx(o.layout, nx, j, k, nx, ny)] = u1;
+        } else if (mb_max) {
+            u1 = flux_lr(K[c], K[c + 1], H[c], H[c + 1], dx);
         }
-        if (j < ny - 1) v1 = -hm_vel(K[c], K[c + nx]) * (H[c + nx] - H[c]) / dx;
-        else {
+        if (j == ny - 1) {
             v1 = face_max_bnd(H, K, c, c - (size_t)(ny - 1) * nx, bc.type[3], bc.value[3], dx);
             o.V[v_idx(o.layout, i, ny, k, nx, ny)] = v1;
+        } else if (mb_max) {
+            v1 = flux_lr(K[c], K[c + nx], H[c], H[c + nx], dx);
         }
-        if (k < nz - 1) w1 = -hm_vel(K[c], K[c + nxy]) * (H[c + nxy] - H[c]) / dx;
-        else {
+        if (k == nz - 1) {
             w1 = face_max_bnd(H, K, c, c - (size_t)(nz - 1) * nxy, bc.type[5], bc.value[5], dx);
             o.W[w_idx(o.layout, i, j, nz, nx, ny)] = w1;
+        } else if (mb_max) {
+            w1 = flux_lr(K[c], K[c + nxy], H[c], H[c + nxy], dx);
         }
         if (mb_max) {
             const double d = ((u1 - u0) + (v1 - v0) + (w1 - w0)) * A;
