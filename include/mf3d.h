@@ -126,6 +126,11 @@ int mf3d_head_solver_create(const mf3d_grid* grid, const mf3d_bc* bc, const mf3d
                             void* stream, mf3d_head_solver** out);
 int mf3d_head_solver_destroy(mf3d_head_solver* s);
 int mf3d_head_solver_num_levels(const mf3d_head_solver* s);
+/* The coarse end of a single solve's V-cycle: its first level (*first_level) and the CTAs of
+ * the thread-block cluster that runs it (*cluster_ctas; 0 when one CTA runs the levels of at
+ * most 4096 cells).  The reference recurses level by level (src/multigrid/cycle/v_cycle.cu:36-74);
+ * this reports how the levels below the streamed ones are grouped into one launch. */
+int mf3d_head_solver_coarse_info(const mf3d_head_solver* s, int* first_level, int* cluster_ctas);
 /* Bytes of device memory the solver holds. */
 long long mf3d_head_solver_device_bytes(const mf3d_head_solver* s);
 

@@ -154,6 +154,14 @@ class HeadSolver:
         return lib().mf3d_head_solver_num_levels(self._h)
 
     @property
+    def coarse_info(self) -> tuple:
+        """(first level of the coarse-end kernel of a single solve, CTAs of its thread-block
+        cluster; 0 when one CTA runs the levels of at most 4096 cells)."""
+        first, ctas = C.c_int(0), C.c_int(0)
+        check(lib().mf3d_head_solver_coarse_info(self._h, C.byref(first), C.byref(ctas)))
+        return first.value, ctas.value
+
+    @property
     def device_bytes(self) -> int:
         return lib().mf3d_head_solver_device_bytes(self._h)
 

@@ -60,6 +60,7 @@ SIGNATURES = {
     "mf3d_head_solver_create": ([_G, _B, C.POINTER(SolverConfig), _P, C.POINTER(_P)], C.c_int),
     "mf3d_head_solver_destroy": ([_P], C.c_int),
     "mf3d_head_solver_num_levels": ([_P], C.c_int),
+    "mf3d_head_solver_coarse_info": ([_P, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
     "mf3d_head_solver_device_bytes": ([_P], C.c_longlong),
     "mf3d_head_solver_set_K": ([_P, _P], C.c_int),
     "mf3d_head_solve": ([_P, _P, _P, C.POINTER(SolveResult)], C.c_int),

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "../../include/mf3d.h"
+#include "kernels_coarse.cuh"
 #include "kernels_kfield.cuh"
 #include "kernels_mg.cuh"
 #include "kernels_nn.cuh"
@@ -40,6 +41,8 @@ static thread_local std::string g_err;
 
 // Shared memory of the one-CTA coarse tail (padded x and b of its levels), at most.
 static constexpr size_t kTailSmemMax = 200 * 1024;
+// ... and of one CTA of the cluster kernel (x, b and the weights of its slabs)
+static constexpr size_t kCoarseSmemMax = 224 * 1024;
 
 // Device-time limit of one solve by default: the PCG loop stops with status 3 after this long
 // (mf3d_head_solver_set_time_budget changes it per solver).
@@ -414,15 +417,169 @@ static SpMaps make_sp_maps(const Geom& g, const T* x, const T* b, const LevelOp<
     return m;
 }
 
+// ---- the coarse levels in one thread-block cluster (kernels_coarse.cuh) ----
+struct CoarsePlan {
+    int Lc = -1; // first level of the cluster kernel; -1: the one-CTA tail serves the coarse end
+    int cn = 0;  // CTAs of the cluster
+    size_t smem = 0;
+    CoarseArgs a{}; // weights unset
+};
+
+// Shared-memory layout of levels Lc .. coarsest with cn CTAs; false when a level does not qualify
+// or the layout does not fit.
+static bool coarse_layout(const std::vector<Geom>& G, const std::vector<LevelOp<double>>& op, int Lc, int cn,
+                          CoarsePlan& p) {
+    const int nl = (int)G.size(), nlev = nl - Lc;
+    if (nlev < 1 || nlev > TAIL2_MAX_LEVELS) return false;
+    CoarseArgs a{};
+    a.nlev = nlev;
+    int ncl = 0;
+    for (int l = Lc; l < nl; ++l) {
+        if (G[l].n > (size_t)CT_MAX_CELLS) return false;
+        if ((op[l].per_x && G[l].nx % 2) || (op[l].per_y && G[l].ny % 2) || (op[l].per_z && G[l].nz % 2)) return false;
+        if (G[l].n > (size_t)CT_LOCAL_MAX) {
+            if (ncl != l - Lc) return false; // clustered levels come first
+            ++ncl;
+        }
+    }
+    a.ncl = ncl;
+    const int last = Lc + ncl - 1; // last clustered level
+    int units = 1;
+    if (ncl > 0) {
+        units = last + 1 < nl ? G[last + 1].nz : G[last].nz;
+        if (units < cn) return false;
+    } else if (cn != 1) {
+        return false;
+    }
+    a.units = units;
+    size_t off = 0;
+    for (int l = Lc; l < nl; ++l) {
+        CLevel& L = a.L[l - Lc];
+        L.nx = G[l].nx;
+        L.ny = G[l].ny;
+        L.nz = G[l].nz;
+        L.n = (int)G[l].n;
+        L.per_x = op[l].per_x;
+        L.per_y = op[l].per_y;
+        L.per_z = op[l].per_z;
+        L.clustered = l <= last;
+        if (L.clustered) {
+            L.shift = last + 1 < nl ? last + 1 - l : last - l;
+            if (((long long)units << L.shift) != L.nz) return false;
+            L.pmax = ((units + cn - 1) / cn) << L.shift;
+        } else {
+            L.shift = 0;
+            L.pmax = L.nz;
+        }
+        L.hcap = (L.nx + 1) / 2 * L.ny * L.pmax;
+        L.xoff = (int)off;
+        off += (size_t)(L.nx + 2) * (L.ny + 2) * (L.pmax + 2);
+        L.boff = (int)off;
+        off += (size_t)2 * L.hcap;
+        L.woff = (int)off;
+        off += (size_t)16 * L.hcap;
+        L.fhx = make_fdiv((L.nx + 1) / 2);
+        L.fnx = make_fdiv(L.nx);
+        L.fny = make_fdiv(L.ny);
+    }
+    {
+        const CLevel& C = a.L[nlev - 1];
+        if (!C.clustered && C.n <= CT_MAP_MAX) { // coarsest level solved by its map
+            a.moff = (int)off;
+            off += (size_t)C.n * 2 * C.hcap;
+        } else {
+            a.moff = -1;
+        }
+    }
+    if (off * sizeof(double) > kCoarseSmemMax) return false;
+    p.a = a;
+    p.smem = off * sizeof(double);
+    p.cn = cn;
+    p.Lc = Lc;
+    return true;
+}
+
+static void coarse_kernel_attrs() {
+    static std::once_flag once;
+    std::call_once(once, [] {
+        MF3D_CK(cudaFuncSetAttribute(coarse_cluster_kernel<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kCoarseSmemMax));
+        MF3D_CK(cudaFuncSetAttribute(coarse_cluster_kernel<double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)kCoarseSmemMax));
+        MF3D_CK(cudaFuncSetAttribute(coarse_cluster_kernel<double, double>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCoarseSmemMax));
+    });
+}
+
+// whether a cluster of cn CTAs with this much shared memory can run on the device
+static bool coarse_cluster_fits(int cn, size_t smem) {
+    coarse_kernel_attrs();
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)cn);
+    cfg.blockDim = dim3(CT_NT);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cn;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int nc = 0;
+    const cudaError_t e = cudaOccupancyMaxActiveClusters(&nc, coarse_cluster_kernel<double, double>, &cfg);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return nc >= 1;
+}
+
+// The lowest first level (most levels) for which the cluster kernel works, with the largest
+// cluster (a power of two, at most CT_MAX_CLUSTER) that fits; Lc = -1 when none does.
+// MF3D_NO_CLUSTER_TAIL=1 keeps the one-CTA tail.
+static CoarsePlan plan_coarse(const std::vector<Geom>& G, const std::vector<LevelOp<double>>& op, int Lt) {
+    CoarsePlan best;
+    if (std::getenv("MF3D_NO_CLUSTER_TAIL")) return best;
+    const int nl = (int)G.size();
+    int lo = nl - 1;
+    while (lo > 0 && G[lo - 1].n <= (size_t)CT_MAX_CELLS) --lo;
+    for (int Lc = lo; Lc <= Lt && Lc < nl; ++Lc)
+        for (int cn = CT_MAX_CLUSTER; cn >= 1; cn /= 2) {
+            CoarsePlan p;
+            if (coarse_layout(G, op, Lc, cn, p) && coarse_cluster_fits(cn, p.smem)) return p;
+        }
+    return best;
+}
+
+template <class TI, class TO>
+static void launch_coarse(cudaStream_t s, const CoarsePlan& p, const CoarseArgs& a, const TI* b_in, TO* x_out) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)p.cn);
+    cfg.blockDim = dim3(CT_NT);
+    cfg.dynamicSmemBytes = p.smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)p.cn;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    MF3D_CK(cudaLaunchKernelEx(&cfg, coarse_cluster_kernel<TI, TO>, a, b_in, x_out));
+    MF3D_LAUNCH_CK();
+}
+
 template <class T, class TC> class VCycle : public VCycleBase {
   public:
     // b0: level-0 right-hand side in the V-cycle's type (the PCG residual or its FP32 copy);
     // r64: the FP64 residual (dot products, and the right-hand side when the whole V-cycle is
     // the coarse tail).
-    VCycle(const std::vector<Geom>& G, int Lt, const mf3d_bc& bc, bool pin, int pre, int post, int coarse,
-           const std::vector<LevelOp<double>>& op64, Scratch scr, const T* b0, const double* r64, bool allow_tma)
-        : G_(G), Lt_(Lt), bc_(bc), pin_(pin), pre_(pre), post_(post), coarse_(coarse), op64_(op64), scr_(scr),
-          b0_(b0), r64_(r64) {
+    // cp: the cluster kernel's plan for single solves (cp.Lc <= Lt), or cp.Lc = -1
+    VCycle(const std::vector<Geom>& G, int Lt, const CoarsePlan& cp, const mf3d_bc& bc, bool pin, int pre, int post,
+           int coarse, const std::vector<LevelOp<double>>& op64, Scratch scr, const T* b0, const double* r64,
+           bool allow_tma)
+        : G_(G), Lt_(Lt), cp_(cp), bc_(bc), pin_(pin), pre_(pre), post_(post), coarse_(coarse), op64_(op64),
+          scr_(scr), b0_(b0), r64_(r64) {
         const int nl = (int)G.size();
         ops_.resize(Lt);
         coef_.resize(Lt);
@@ -521,12 +678,38 @@ template <class T, class TC> class VCycle : public VCycleBase {
             tail_.pre = pre;
             tail_.post = post;
             tail_.coarse_iters = coarse;
+            // weights of every level either coarse kernel serves: [Lw, coarsest)
+            Lw_ = cp_.Lc >= 0 ? std::min(cp_.Lc, Lt) : Lt;
             size_t wtot = 0;
-            for (int l = Lt; l < nl; ++l) wtot += 8 * G[l].n;
+            for (int l = Lw_; l < nl; ++l) wtot += 8 * G[l].n;
             tail_w_.reset(new DevMem(wtot * sizeof(double)));
             bytes_ += tail_w_->bytes;
+            {
+                size_t wo = 0;
+                for (int l = Lw_; l < nl; ++l) {
+                    if (cp_.Lc >= 0 && l >= cp_.Lc) cp_.a.L[l - cp_.Lc].w = tail_w_->as<double>() + wo;
+                    wo += 8 * G[l].n;
+                }
+                if (cp_.Lc >= 0) {
+                    cp_.a.pre = pre;
+                    cp_.a.post = post;
+                    cp_.a.coarse_iters = coarse;
+                    cp_.a.M = nullptr;
+                    if (cp_.a.moff >= 0) {
+                        const CLevel& C = cp_.a.L[cp_.a.nlev - 1];
+                        cmap_.reset(new DevMem((size_t)C.n * 2 * C.hcap * sizeof(double)));
+                        bytes_ += cmap_->bytes;
+                        cp_.a.M = cmap_->as<double>();
+                    }
+                    if (cp_.Lc > 0 && cp_.Lc < Lt) {
+                        ctail_out_.reset(new DevMem(G[cp_.Lc].n * sizeof(T)));
+                        bytes_ += ctail_out_->bytes;
+                    }
+                }
+            }
             int off = 0;
             size_t woff = 0;
+            for (int l = Lw_; l < Lt; ++l) woff += 8 * G[l].n;
             for (int l = Lt; l < nl; ++l) {
                 TailLevel& T2 = tail_.L[l - Lt];
                 T2.nx = G[l].nx;
@@ -584,8 +767,17 @@ template <class T, class TC> class VCycle : public VCycleBase {
     void build_coefs(cudaStream_t s, const std::vector<const double*>& Klev) override {
         if (!std::is_same<TC, double>::value)
             for (int l = 0; l < Lt_; ++l) launch_faces<TC>(s, G_[l], Klev[l], bc_, scale_[l], ops_[l]);
-        for (int l = Lt_; l < (int)G_.size(); ++l) {
-            tail_weights_kernel<<<grid1d(G_[l].n, 256), 256, 0, s>>>(op64_[l], (double*)tail_.L[l - Lt_].w);
+        size_t wo = 0;
+        for (int l = Lw_; l < (int)G_.size(); ++l) {
+            tail_weights_kernel<<<grid1d(G_[l].n, 256), 256, 0, s>>>(op64_[l], tail_w_->as<double>() + wo);
+            MF3D_LAUNCH_CK();
+            wo += 8 * G_[l].n;
+        }
+        if (cmap_) { // the coarsest level's sweeps as a matrix, one column per cell
+            const int nl = (int)G_.size();
+            const CLevel& C = cp_.a.L[cp_.a.nlev - 1];
+            MF3D_CK(cudaMemsetAsync(cmap_->p, 0, cmap_->bytes, s));
+            coarse_map_kernel<<<C.n, 64, 0, s>>>(tail_.L[nl - 1 - Lt_], C, coarse_, cmap_->as<double>());
             MF3D_LAUNCH_CK();
         }
     }
@@ -597,9 +789,12 @@ template <class T, class TC> class VCycle : public VCycleBase {
     void run(cudaStream_t s, void* zv, double* rho_out) override {
         T* z = (T*)zv;
         const int nl = (int)G_.size();
-        std::vector<const T*> cur(Lt_ + 1, nullptr), fin(Lt_ + 1, nullptr);
+        // levels above the coarse kernel: the cluster kernel's for single solves, the one-CTA
+        // tail's for batched ones
+        const int Lb = coarse_start();
+        std::vector<const T*> cur(Lb + 1, nullptr), fin(Lb + 1, nullptr);
         // ---- down ----
-        for (int l = 0; l < Lt_; ++l) {
+        for (int l = 0; l < Lb; ++l) {
             T* bc_next = (T*)bl_[l + 1]->p;
             const T* c = nullptr;
             for (int sw = 1; sw <= pre_; ++sw) {
@@ -617,18 +812,18 @@ template <class T, class TC> class VCycle : public VCycleBase {
             if (pre_ == 0) restrict_b(s, l, bc_next);
             cur[l] = c;
         }
-        // ---- tail (coarsest levels in one CTA, FP64) ----
+        // ---- coarse end (FP64): one cluster, or one CTA ----
         const T* e_below = nullptr;
-        if (Lt_ < nl) {
-            T* out = (Lt_ == 0) ? z : (T*)tail_out_->p;
+        if (Lb < nl) {
+            T* out = coarse_out(z);
             launch_tail(s, out);
             e_below = out;
-            if (Lt_ == 0 && rho_out) dot_rz(s, z, G_[0].n, rho_out);
+            if (Lb == 0 && rho_out) dot_rz(s, z, G_[0].n, rho_out);
         }
         // ---- up ----
-        for (int l = Lt_ - 1; l >= 0; --l) {
+        for (int l = Lb - 1; l >= 0; --l) {
             const T* c = cur[l];
-            const T* e = (l + 1 == Lt_) ? e_below : fin[l + 1];
+            const T* e = (l + 1 == Lb) ? e_below : fin[l + 1];
             for (int sw = 1; sw <= post_; ++sw) {
                 const bool last = sw == post_;
                 T* out = (l == 0 && last) ? z : other(l, c);
@@ -653,13 +848,14 @@ template <class T, class TC> class VCycle : public VCycleBase {
         T* z = (T*)zv;
         const int nl = (int)G_.size();
         out.push_back(timing("vcycle_total", tm.mean_ms(reps, [&] { run(tm.s, zv, rho_out); }), 0.0, 1));
-        if (Lt_ >= 1) {
+        const int Lb = coarse_start();
+        if (Lb >= 1) {
             const double n = (double)G_[0].n, et = sizeof(T), ec = sizeof(TC);
             const double coef = 3.0 * n * ec, nc = n / 8.0;
             T* xa = (T*)xa_[0]->p;
             T* xb = (T*)xb_[0]->p;
             T* bc1 = (T*)bl_[1]->p;
-            const T* e1 = (Lt_ == 1) ? (const T*)tail_out_->p : (const T*)xa_[1]->p;
+            const T* e1 = (coarse_start() == 1) ? (const T*)coarse_out(z) : (const T*)xa_[1]->p;
             const int pre_extra = std::max(0, pre_ - 2), post_extra = std::max(0, post_ - 2);
             const char* tag = pair_[0] ? "pair" : (tma_[0] ? "tma" : "ldg");
             char nm[40];
@@ -700,7 +896,7 @@ template <class T, class TC> class VCycle : public VCycleBase {
                     sweep(tm.s, 0, xa, z, e1, nullptr, post_ == 1 ? (M_PROLONG | M_DOT) : M_DOT, rho_out);
                 }), et * n + et * n + coef + et * n + 8.0 * n + (post_ == 1 ? et * nc : 0.0), 1));
             }
-            for (int l = 1; l < Lt_; ++l) {
+            for (int l = 1; l < Lb; ++l) {
                 std::snprintf(nm, sizeof(nm), "sweep_l%d_plain_%s", l, pair_[l] ? "pair" : (tma_[l] ? "tma" : "ldg"));
                 T* a = (T*)xa_[l]->p;
                 T* b = (T*)xb_[l]->p;
@@ -709,9 +905,10 @@ template <class T, class TC> class VCycle : public VCycleBase {
                                      3.0 * et * nn + 3.0 * nn * ec, pre_ + post_));
             }
         }
-        if (Lt_ < nl) {
-            T* outp = (Lt_ == 0) ? z : (T*)tail_out_->p;
-            out.push_back(timing("coarse_tail", tm.mean_ms(reps, [&] { launch_tail(tm.s, outp); }), 0.0, 1));
+        if (Lb < nl) {
+            T* outp = coarse_out(z);
+            out.push_back(timing(cluster_on() ? "coarse_cluster" : "coarse_tail",
+                                 tm.mean_ms(reps, [&] { launch_tail(tm.s, outp); }), 0.0, 1));
         }
     }
 
@@ -722,7 +919,25 @@ template <class T, class TC> class VCycle : public VCycleBase {
 
     T* other(int l, const T* c) const { return (c == (const T*)xa_[l]->p) ? (T*)xb_[l]->p : (T*)xa_[l]->p; }
 
+    // the cluster kernel serves this solve's coarse end (single solves with a plan)
+    bool cluster_on() const { return cp_.Lc >= 0 && !rec_tail_ && !rec_; }
+    int coarse_start() const { return cluster_on() ? cp_.Lc : Lt_; }
+    // where the coarse end writes its correction: z when it is the whole V-cycle
+    T* coarse_out(T* z) const {
+        const int Lb = coarse_start();
+        if (Lb == 0) return z;
+        if (cluster_on() && Lb < Lt_) return (T*)ctail_out_->p;
+        return (T*)tail_out_->p;
+    }
+
     void launch_tail(cudaStream_t s, T* out) {
+        if (cluster_on()) {
+            if (cp_.Lc == 0)
+                launch_coarse<double, T>(s, cp_, cp_.a, r64_, out);
+            else
+                launch_coarse<T, T>(s, cp_, cp_.a, (const T*)bl_[cp_.Lc]->p, out);
+            return;
+        }
         if (rec_tail_) { // batched solve: record only (the batch needs a level above the tail)
             if (Lt_ == 0) throw Error(MF3D_E_INVALID, "batched solve: the whole hierarchy fits the coarse tail");
             rec_tail_->a = tail_;
@@ -986,6 +1201,7 @@ template <class T, class TC> class VCycle : public VCycleBase {
 
     std::vector<Geom> G_;
     int Lt_;
+    CoarsePlan cp_; // the cluster kernel (cp_.Lc >= 0) for single solves
     mf3d_bc bc_;
     bool pin_;
     int pre_, post_, coarse_;
@@ -1012,8 +1228,9 @@ template <class T, class TC> class VCycle : public VCycleBase {
     std::vector<std::array<SpMaps, 2>> pmaps_; // their tensor maps, x read from xa / xb
     int n_pair_ = 0;
     int pocc_[16] = {}, pocc_tm_[16] = {}; // resident x-pair-sweep CTAs per SM, by mode
-    std::unique_ptr<DevMem> tail_out_, tail_w_;
+    std::unique_ptr<DevMem> tail_out_, tail_w_, ctail_out_, cmap_;
     Tail2Args tail_{};
+    int Lw_ = 0; // first level with FP64 weights
     size_t tail_smem_ = 0;
     size_t bytes_ = 0;
 };
@@ -1084,9 +1301,12 @@ class HeadSolver {
         // FP64 V-cycle.
         op64_.resize(nl);
         coef64_.resize(nl);
+        for (int l = 0; l < nl; ++l) op64_[l] = make_op<double>(G_[l], bc, pin_, 1.0);
+        // the coarse levels of single solves in one thread-block cluster, where they qualify
+        cplan_ = plan_coarse(G_, op64_, Lt_);
+        const int Lw = cplan_.Lc >= 0 ? std::min(cplan_.Lc, Lt_) : Lt_;
         for (int l = 0; l < nl; ++l) {
-            op64_[l] = make_op<double>(G_[l], bc, pin_, 1.0);
-            if (l == 0 || l >= Lt_ || cfg.precision == MF3D_PREC_FP64) {
+            if (l == 0 || l >= Lw || cfg.precision == MF3D_PREC_FP64) {
                 coef64_[l].reset(new CoefStore());
                 coef64_[l]->build<double>(G_[l], sizeof(double), op64_[l]);
                 bytes_ += coef64_[l]->mem.bytes;
@@ -1132,13 +1352,13 @@ class HeadSolver {
             bytes_ += r32_.bytes;
         }
         if (prec == MF3D_PREC_FP64)
-            vc_.reset(new VCycle<double, double>(G_, Lt_, bc, pin_, cfg.mg_pre_smooth, cfg.mg_post_smooth,
+            vc_.reset(new VCycle<double, double>(G_, Lt_, cplan_, bc, pin_, cfg.mg_pre_smooth, cfg.mg_post_smooth,
                                                  cfg.mg_coarse_iters, op64_, scr, r_.as<double>(), r_.as<double>(), tma));
         else if (prec == MF3D_PREC_FP32)
-            vc_.reset(new VCycle<float, float>(G_, Lt_, bc, pin_, cfg.mg_pre_smooth, cfg.mg_post_smooth,
+            vc_.reset(new VCycle<float, float>(G_, Lt_, cplan_, bc, pin_, cfg.mg_pre_smooth, cfg.mg_post_smooth,
                                                cfg.mg_coarse_iters, op64_, scr, r32_.as<float>(), r_.as<double>(), tma));
         else if (prec == MF3D_PREC_BF16)
-            vc_.reset(new VCycle<float, __nv_bfloat16>(G_, Lt_, bc, pin_, cfg.mg_pre_smooth, cfg.mg_post_smooth,
+            vc_.reset(new VCycle<float, __nv_bfloat16>(G_, Lt_, cplan_, bc, pin_, cfg.mg_pre_smooth, cfg.mg_post_smooth,
                                                        cfg.mg_coarse_iters, op64_, scr, r32_.as<float>(),
                                                        r_.as<double>(), tma));
         else
@@ -1168,6 +1388,10 @@ class HeadSolver {
 
     int num_levels() const { return (int)G_.size(); }
     long long device_bytes() const { return (long long)bytes_; }
+    void coarse_info(int* first, int* ctas) const {
+        if (first) *first = cplan_.Lc >= 0 ? cplan_.Lc : Lt_;
+        if (ctas) *ctas = cplan_.Lc >= 0 ? cplan_.cn : 0;
+    }
 
     void set_K(const double* K) {
         if (!K) throw Error(MF3D_E_INVALID, "K is null");
@@ -1436,6 +1660,7 @@ class HeadSolver {
     bool have_K_ = false;
     std::vector<Geom> G_;
     int Lt_ = 0;
+    CoarsePlan cplan_;
     cudaStream_t stream_ = nullptr, own_stream_ = nullptr;
     std::vector<LevelOp<double>> op64_;
     std::vector<std::unique_ptr<CoefStore>> coef64_;
@@ -1587,6 +1812,12 @@ int mf3d_head_solver_destroy(mf3d_head_solver* s) {
 int mf3d_head_solver_num_levels(const mf3d_head_solver* s) { return s ? s->impl->num_levels() : MF3D_E_INVALID; }
 
 long long mf3d_head_solver_device_bytes(const mf3d_head_solver* s) { return s ? s->impl->device_bytes() : -1; }
+
+int mf3d_head_solver_coarse_info(const mf3d_head_solver* s, int* first_level, int* cluster_ctas) {
+    if (!s) return MF3D_E_INVALID;
+    s->impl->coarse_info(first_level, cluster_ctas);
+    return MF3D_OK;
+}
 
 int mf3d_head_solver_set_K(mf3d_head_solver* s, const double* K) {
     return guard([&] {

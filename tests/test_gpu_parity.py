@@ -169,6 +169,45 @@ def test_vcycle_vs_oracle(mf3d, oracle_mod, shape, levels, pre, post, coarse, ca
     assert _rel(_np(z), zo) < 1e-10
 
 
+@pytest.mark.parametrize("shape,levels", [((64, 64, 64), 5), ((24, 16, 52), 3), ((32, 32, 32), 4),
+                                          ((64, 48, 32), 4)])
+@pytest.mark.parametrize("bcname", ["darcy", "periodic_yz"])
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_cluster_coarse_end_matches_one_cta_tail(mf3d, monkeypatch, shape, levels, bcname, prec):
+    """The coarse end in one thread-block cluster (levels of up to 32^3 cells in z slabs over
+    the cluster's CTAs, FP64) against the same V-cycle with the one-CTA tail and x-pair sweeps
+    above it: equal to rounding in FP64 (1e-12), to FP32 rounding of the levels it replaces
+    in the FP32 V-cycle (1e-5)."""
+    M = mf3d
+    rng = np.random.default_rng(zlib.crc32(repr((shape, levels, bcname)).encode()))
+    K = np.exp(rng.normal(size=shape))
+    r = rng.normal(size=shape)
+    g = M.Grid3D(shape[2], shape[1], shape[0], 1.0)
+    if bcname == "darcy":
+        bc = M.BCSpec.darcy_x()
+    else:
+        bc = _bcs(M, [D, D, P, P, P, P], [1.0, 0.0, 0, 0, 0, 0])
+    P_ = {"fp64": M.PREC_FP64, "fp32": M.PREC_FP32}[prec]
+    cfg = M.HeadSolveConfig(mg_levels=levels, precision=P_)
+    z = {}
+    for mode in ("cluster", "tail"):
+        if mode == "tail":
+            monkeypatch.setenv("MF3D_NO_CLUSTER_TAIL", "1")
+        s = M.HeadSolver(g, bc, cfg)
+        first, ctas = s.coarse_info
+        if mode == "cluster":
+            assert ctas >= 2, (first, ctas)
+        else:
+            assert ctas == 0
+        s.set_K(_t(K))
+        zz = _t(np.zeros(shape))
+        s.vcycle(_t(r), zz)
+        z[mode] = _np(zz)
+        s.close()
+        monkeypatch.delenv("MF3D_NO_CLUSTER_TAIL", raising=False)
+    assert _rel(z["cluster"], z["tail"]) < (1e-12 if prec == "fp64" else 1e-5)
+
+
 def _lognormal(shape, sigma, seed):
     return np.exp(sigma * np.random.default_rng(seed).normal(size=shape))
 
