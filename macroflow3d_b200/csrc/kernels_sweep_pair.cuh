@@ -148,6 +148,7 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
     static_assert((MODE & M_RESID) == 0, "the residual runs in a kernel of its own");
     using G = SpGeom<T, TM>;
     constexpr int ST = G::ST, W = G::W, HX = G::HX, NP = G::NP, TX = G::TX;
+    constexpr int QS = 32; // cells between the pairs of one lane (16 lanes x one pair each)
     extern __shared__ __align__(128) unsigned char sp_sm_raw[];
     // slots start on a 128-byte boundary of the shared window (TMA destinations)
     unsigned char* const sp_sm =
@@ -376,8 +377,9 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
 
         if (role == 0) {
             // =============== tile pairs: red of plane t and black of plane t-1 ===============
-            // NP pairs per thread, side by side in one row: pair q starts at cell i0 + 2 (NP lo + q)
-            const int pj = j0 + tyr, pi0 = i0 + 2 * NP * lo;
+            // NP pairs per thread in one row: pair q starts at cell i0 + 2 lo + QS q, so that the
+            // 16 lanes of a row read and write consecutive pairs
+            const int pj = j0 + tyr, pi0 = i0 + 2 * lo;
             const int wj = pj < ny ? pj : -1; // never wrapped
             const int fx = (pj - j0 + 2) * W + (pi0 - i0 + HX), fc = fx - W;
             bool pin[NP];
@@ -385,13 +387,13 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
             int cxl_off[NP], cyd_off[NP];
 #pragma unroll
             for (int q = 0; q < NP; ++q) {
-                const int pi = pi0 + 2 * q;
+                const int pi = pi0 + QS * q;
                 pin[q] = pi < nx && wj >= 0;
                 gxy[q] = pin[q] ? (long long)pi + (long long)nx * wj : 0;
                 // the -x face of cell pi - 1 and the -y faces of the pair: from the boundary-face
                 // buffers where the TMA form stages them, else from the cx / cy slots
-                cxl_off[q] = (TM && i0 == 0 && pi == 0) ? OBX + (pj - j0 + G::BXS) : OCX + fc + 2 * q - 1;
-                cyd_off[q] = (TM && j0 == 0 && pj == 0) ? OBY + (pi - i0 + HX) : OCY + fx + 2 * q - W;
+                cxl_off[q] = (TM && i0 == 0 && pi == 0) ? OBX + (pj - j0 + G::BXS) : OCX + fc + QS * q - 1;
+                cyd_off[q] = (TM && j0 == 0 && pj == 0) ? OBY + (pi - i0 + HX) : OCY + fx + QS * q - W;
             }
             auto issue = [&](int p) {
                 if constexpr (TM) {
@@ -422,11 +424,11 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
             double2 r64n[NP];
 #pragma unroll
             for (int q = 0; q < NP; ++q) {
-                const int pi = pi0 + 2 * q;
-                const P2<T> xp0 = take(0, fx + 2 * q, corr(pin[q], pi, wj, P0)); // x(P0): own column only
-                const P2<T> xp1 = take(1, fx + 2 * q, corr(pin[q], pi, wj, P0 + 1)); // x(P0 + 1), published
+                const int pi = pi0 + QS * q;
+                const P2<T> xp0 = take(0, fx + QS * q, corr(pin[q], pi, wj, P0)); // x(P0): own column only
+                const P2<T> xp1 = take(1, fx + QS * q, corr(pin[q], pi, wj, P0 + 1)); // x(P0 + 1), published
                 en[q] = corr(pin[q], pi, wj, P0 + 2); // correction of the pair in plane t + 1
-                czp1[q] = sp_ld2<TC>(cs0 + OCZ + fc + 2 * q);
+                czp1[q] = sp_ld2<TC>(cs0 + OCZ + fc + QS * q);
                 czp2[q] = P2<T>{(T)0, (T)0};
                 A[q] = O0 ? xp1.a : xp1.b;
                 B[q] = O0 ? xp0.b : xp0.a;
@@ -444,13 +446,13 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
                 const bool out_ok = q_out >= z0 && q_out < z1;
 #pragma unroll
                 for (int q = 0; q < NP; ++q) {
-                    const int f = fx + 2 * q, g = fc + 2 * q;
+                    const int f = fx + QS * q, g = fc + QS * q;
                     // ---- x of plane t+1 (own column; published for the neighbours with PROL) ----
                     T xnO;
                     if constexpr (PROL) {
                         const P2<T> v = take(sx1, f, en[q]);
                         xnO = O ? v.b : v.a;
-                        en[q] = corr(pin[q], pi0 + 2 * q, wj, t + 2);
+                        en[q] = corr(pin[q], pi0 + QS * q, wj, t + 2);
                     } else if constexpr (ZERO) {
                         xnO = (T)0;
                     } else {
@@ -475,7 +477,7 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
                         const T cyp = O ? cy2p.b : cy2p.a, cym = O ? cyd2.b : cyd2.a;
                         const T czp = O ? cz2.b : cz2.a, czm = O ? czp1[q].b : czp1[q].a;
                         T D = cxm + cxp + cym + cyp + czm + czp;
-                        if (O == 0 && L.pin && pi0 + 2 * q == 0 && pj == 0 && zzero(t)) D *= (T)2; // cell 0 is red
+                        if (O == 0 && L.pin && pi0 + QS * q == 0 && pj == 0 && zzero(t)) D *= (T)2; // cell 0 is red
                         const T sum = cxp * xe + cxm * xw + cyp * xnv + cym * xsv + czp * xnO + czm * B[q];
                         const T bb = O ? b2.b : b2.a;
                         if (pin[q] && zin(t)) red = divide(sum - bb * dx2, D);
@@ -531,7 +533,7 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
             // =============== ring pairs / cells: red of plane t only ===============
             // ring-row lanes: NP pairs side by side; ring-column lanes: one cell (its side pair)
             int pj, pi0, side = -1;
-            if (role == 1) pj = hi ? j0 + SP_TY : j0 - 1, pi0 = i0 + 2 * NP * lo;
+            if (role == 1) pj = hi ? j0 + SP_TY : j0 - 1, pi0 = i0 + 2 * lo;
             else side = hi, pj = j0 + lo, pi0 = hi ? i0 + TX : i0 - 2;
             const int npair = role == 1 ? NP : 1;
             const int wj = wrap_or_out(pj, ny, L.per_y);
@@ -560,7 +562,7 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
             long long gxy[NP], gxy2[NP], gcy2[NP];
 #pragma unroll
             for (int q = 0; q < NP; ++q) {
-                const int pi = pi0 + 2 * q;
+                const int pi = pi0 + QS * q;
                 wi[q] = wrap_or_out(pi, nx, L.per_x);
                 pin[q] = q < npair && wi[q] >= 0 && wj >= 0;
                 gxy[q] = pin[q] ? (long long)wi[q] + (long long)nx * wj : 0;
@@ -568,8 +570,8 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
                 gxy2[q] = pin2[q] ? (long long)wi[q] + (long long)nx * wj2 : 0;
                 gcy2[q] = (wi[q] >= 0 && wcy2 >= 0) ? (long long)wi[q] + (long long)nx * wcy2 : 0;
                 cx_bnd[q] = pi == -2 && !L.per_x;
-                cxl_off[q] = (TM && i0 == 0 && pi == 0) ? OBX + (pj - j0 + G::BXS) : OCX + fc + 2 * q - 1;
-                cyd_off[q] = (TM && j0 == 0 && pj == 0) ? OBY + (pi - i0 + HX) : OCY + fx + 2 * q - W;
+                cxl_off[q] = (TM && i0 == 0 && pi == 0) ? OBX + (pj - j0 + G::BXS) : OCX + fc + QS * q - 1;
+                cyd_off[q] = (TM && j0 == 0 && pj == 0) ? OBY + (pi - i0 + HX) : OCY + fx + QS * q - W;
             }
             auto issue = [&](int p) {
                 if constexpr (!TM) { // (one pair per lane: NP == 1 in this form)
@@ -630,12 +632,12 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
                 xprev[q] = xcur[q] = czp1[q] = P2<T>{(T)0, (T)0};
                 en[q] = en2[q] = (T)0;
                 if (q >= npair) continue;
-                xprev[q] = take(0, fx + 2 * q, corr(pin[q], wi[q], wj, P0));
-                xcur[q] = take(1, fx + 2 * q, corr(pin[q], wi[q], wj, P0 + 1));
-                if (has2) (void)take(1, fx2 + 2 * q, corr(pin2[q], wi[q], wj2, P0 + 1));
+                xprev[q] = take(0, fx + QS * q, corr(pin[q], wi[q], wj, P0));
+                xcur[q] = take(1, fx + QS * q, corr(pin[q], wi[q], wj, P0 + 1));
+                if (has2) (void)take(1, fx2 + QS * q, corr(pin2[q], wi[q], wj2, P0 + 1));
                 en[q] = corr(pin[q], wi[q], wj, P0 + 2);
                 en2[q] = has2 ? corr(pin2[q], wi[q], wj2, P0 + 2) : (T)0;
-                czp1[q] = sp_ld2<TC>(cs0 + OCZ + fc + 2 * q);
+                czp1[q] = sp_ld2<TC>(cs0 + OCZ + fc + QS * q);
             }
             for (int t = z0 - 1; t <= z1; ++t) {
                 if (!sync_step(t + 1, sx1)) {
@@ -649,9 +651,9 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
 #pragma unroll
                 for (int q = 0; q < NP; ++q) {
                     if (q >= npair) break;
-                    const int f = fx + 2 * q, g = fc + 2 * q;
+                    const int f = fx + QS * q, g = fc + QS * q;
                     const P2<T> xnext = take(sx1, f, en[q]);
-                    if (has2) (void)take(sx1, fx2 + 2 * q, en2[q]);
+                    if (has2) (void)take(sx1, fx2 + QS * q, en2[q]);
                     if constexpr (PROL) {
                         en[q] = corr(pin[q], wi[q], wj, t + 2);
                         if (has2) en2[q] = corr(pin2[q], wi[q], wj2, t + 2);
