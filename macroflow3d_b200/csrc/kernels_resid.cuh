@@ -43,17 +43,24 @@ template <class T, class TC> struct RrSlot {
 };
 template <class T, class TC> constexpr size_t rr_smem_bytes() { return RR_NS * sizeof(RrSlot<T, TC>); }
 
-// two consecutive values of type E at p, as T
+// one value / two consecutive values of type E at p, as T
+template <class T, class E> __device__ __forceinline__ T rr_one(const E* p) {
+    if constexpr (std::is_same<E, __nv_bfloat16>::value) return (T)__bfloat162float(*p);
+    else return (T)*p;
+}
 template <class T, class E> __device__ __forceinline__ void rr_pair(const E* p, T& a, T& b) {
-    a = (T)p[0];
-    b = (T)p[1];
+    a = rr_one<T>(p);
+    b = rr_one<T>(p + 1);
 }
 
 template <class T, class TC>
 __global__ void __launch_bounds__(256, MF3D_RR_MINB)
     resid_restrict_staged_kernel(const LevelOp<TC> L, const T* __restrict__ x, const T* __restrict__ b,
                                  T* __restrict__ b_coarse, int zchunk) {
-    static_assert(sizeof(T) >= 4 && sizeof(TC) >= 4, "cp.async moves 4, 8 or 16 bytes per copy");
+    // cp.async moves 4, 8 or 16 bytes per copy: a pair of BF16 faces is one 4-byte copy, and the
+    // single -x face of a row (kind 3 below) is loaded one plane ahead and stored by hand
+    static_assert(sizeof(T) >= 4 && (sizeof(TC) >= 4 || std::is_same<TC, __nv_bfloat16>::value),
+                  "FP64 / FP32 coefficients, or BF16 coefficients with FP32 vectors");
     using Slot = RrSlot<T, TC>;
     constexpr int ST = (int)sizeof(T), SC = (int)sizeof(TC);
     extern __shared__ __align__(16) unsigned char rr_sm[];
@@ -114,6 +121,10 @@ __global__ void __launch_bounds__(256, MF3D_RR_MINB)
     }
     long long gO;
     const bool okO = xy_of(i, j, gO);
+    TC face_next = TC(0.0f); // SC == 2, kind 3: the -x face of plane kk + 1, loaded at issue(kk)
+    if constexpr (SC == 2) {
+        if (kindE == 3 && okE && k0 < k1) face_next = cb[cs * (size_t)k0];
+    }
     // one commit group per plane kk: x of the staged cells; b and the faces for kk < k1
     auto issue = [&](int kk) {
         if (kk <= k1) {
@@ -137,8 +148,16 @@ __global__ void __launch_bounds__(256, MF3D_RR_MINB)
                     pmv_cp<2 * SC>(&S.cy[ty + 1][2 * tx], L.cy + c, true);
                     pmv_cp<2 * SC>(&S.cz[ty][2 * tx], L.cz + c, true);
                 }
-                if (kindE == 3) pmv_cp<SC>(Sb + fE, cb + cs * kk, okE);
-                else if (kindE == 4) pmv_cp<2 * SC>(Sb + fE, cb + cs * kk, okE);
+                if (kindE == 3) {
+                    if constexpr (SC == 2) { // store the face fetched one plane ago, fetch the next
+                        *reinterpret_cast<TC*>(Sb + fE) = okE ? face_next : TC(0.0f);
+                        if (okE && kk + 1 < k1) face_next = cb[cs * (size_t)(kk + 1)];
+                    } else {
+                        pmv_cp<SC>(Sb + fE, cb + cs * kk, okE);
+                    }
+                } else if (kindE == 4) {
+                    pmv_cp<2 * SC>(Sb + fE, cb + cs * kk, okE);
+                }
             }
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
@@ -176,7 +195,7 @@ __global__ void __launch_bounds__(256, MF3D_RR_MINB)
         rr_pair<T>(X - RR_XW, xs0, xs1);
         rr_pair<T>(X + RR_XW, xn0, xn1);
         const T xw0 = X[-1], xe1 = X[2];
-        T cxm0 = (T)S.cx[ty][1 + 2 * tx], cxp0, cxp1, cym0, cym1, cyp0, cyp1, czp0, czp1, b0, b1;
+        T cxm0 = rr_one<T>(&S.cx[ty][1 + 2 * tx]), cxp0, cxp1, cym0, cym1, cyp0, cyp1, czp0, czp1, b0, b1;
         rr_pair<T>(&S.cx[ty][2 + 2 * tx], cxp0, cxp1);
         rr_pair<T>(&S.cy[ty][2 * tx], cym0, cym1);
         rr_pair<T>(&S.cy[ty + 1][2 * tx], cyp0, cyp1);

@@ -62,31 +62,36 @@ constexpr int SP_NSX = SP_D + 2; // x planes t-1 .. t+D
 constexpr int SP_NSC = SP_D;     // coefficient planes t .. t+D-1
 
 // Shared-memory layout of one precision and staging form.  Columns i0-HX .. i0+TX+HX-1 (a TMA
-// box starts on a 16-byte boundary); every array of a slot starts on a 128-byte boundary.
-template <class T, bool TM> struct SpGeom {
-    static constexpr int ST = (int)sizeof(T);
-    // x-pairs per thread: two (a quad of cells) in FP32 with TMA staging, where one pair per
-    // thread would move too few bytes per plane step; one otherwise
+// box starts on a 16-byte boundary, for the narrower of the vector and coefficient types);
+// every array of a slot starts on a 128-byte boundary.
+template <class T, class TC, bool TM> struct SpGeom {
+    static constexpr int ST = (int)sizeof(T), SC = (int)sizeof(TC);
+    static constexpr int SMIN = ST < SC ? ST : SC;
+    // x-pairs per thread: two (a quad of cells) with FP32 vectors and TMA staging, where one
+    // pair per thread would move too few bytes per plane step; one otherwise
     static constexpr int NP = (ST == 4 && TM) ? 2 : 1;
     static constexpr int TX = SP_TX * NP; // tile width (cells)
-    static constexpr int HX = TM ? 16 / ST : 2;
+    static constexpr int HX = TM ? 16 / SMIN : 2;
     static constexpr int W = TX + 2 * HX;
-    static constexpr int BXS = TM ? 16 / ST : 2; // the -x face buffer starts at row j0 - BXS
+    static constexpr int BXS = TM ? 16 / SC : 2; // the -x face buffer starts at row j0 - BXS
     static constexpr int BXN = SP_TY + 2 * BXS;
     static constexpr size_t a128(size_t v) { return (v + 127) & ~(size_t)127; }
     static constexpr size_t XSB = a128((size_t)SP_XR * W * ST); // x slot
-    static constexpr size_t CB = a128((size_t)SP_CR * W * ST), CYB = a128((size_t)SP_YR * W * ST);
-    // coefficient slot: b, cx, cy, cz, then the -x faces (bxm) and -y faces (bym) of a tile on
-    // the grid's min faces (TMA form)
-    static constexpr size_t OB = 0, OCX = CB, OCY = 2 * CB, OCZ = 2 * CB + CYB, OBX = 3 * CB + CYB;
-    static constexpr size_t OBY = OBX + a128((size_t)BXN * ST);
-    static constexpr size_t CSB = OBY + a128((size_t)W * ST);
+    // coefficient slot: b (vector type), then cx, cy, cz and the -x faces (bxm) and -y faces
+    // (bym) of a tile on the grid's min faces (TMA form), in the coefficient type
+    static constexpr size_t BB = a128((size_t)SP_CR * W * ST);
+    static constexpr size_t CB = a128((size_t)SP_CR * W * SC), CYB = a128((size_t)SP_YR * W * SC);
+    static constexpr size_t OB = 0, OCX = BB, OCY = BB + CB, OCZ = BB + CB + CYB, OBX = BB + 2 * CB + CYB;
+    static constexpr size_t OBY = OBX + a128((size_t)BXN * SC);
+    static constexpr size_t CSB = OBY + a128((size_t)W * SC);
     static constexpr size_t SMEM = SP_NSX * XSB + SP_NSC * CSB + 128; // + alignment of the base
 };
-template <class T, class TC, bool TM> constexpr size_t sp_smem_bytes() { return SpGeom<T, TM>::SMEM; }
-template <class T, bool TM> constexpr int sp_tx() { return SpGeom<T, TM>::TX; }
+template <class T, class TC, bool TM> constexpr size_t sp_smem_bytes() { return SpGeom<T, TC, TM>::SMEM; }
+template <class T, class TC, bool TM> constexpr int sp_tx() { return SpGeom<T, TC, TM>::TX; }
 // resident CTAs per SM the register budget is cut for
-template <class T, bool TM> constexpr int sp_minb() { return (sizeof(T) == 8 || SpGeom<T, TM>::NP == 2) ? 2 : 3; }
+template <class T, class TC, bool TM> constexpr int sp_minb() {
+    return (sizeof(T) == 8 || SpGeom<T, TC, TM>::NP == 2) ? 2 : 3;
+}
 
 template <class T, class TC> struct SpArgs {
     LevelOp<TC> L;
@@ -122,6 +127,19 @@ template <class T> __device__ __forceinline__ P2<T> sp_ld2(const T* p) {
         return P2<T>{(T)v.x, (T)v.y};
     }
 }
+// a coefficient pair (cells 2m, 2m+1) in the vector type
+template <class T, class TC> __device__ __forceinline__ P2<T> sp_ldc(const TC* p) {
+    if constexpr (std::is_same<TC, __nv_bfloat16>::value) {
+        const float2 v = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+        return P2<T>{(T)v.x, (T)v.y};
+    } else {
+        return sp_ld2<T>(reinterpret_cast<const T*>(p));
+    }
+}
+template <class T, class TC> __device__ __forceinline__ T sp_c1(const TC* p) {
+    if constexpr (std::is_same<TC, __nv_bfloat16>::value) return (T)__bfloat162float(*p);
+    else return (T)*p;
+}
 template <class T> __device__ __forceinline__ void sp_st2(T* p, T a, T b) {
     if constexpr (sizeof(T) == 8) *reinterpret_cast<double2*>(p) = make_double2(a, b);
     else *reinterpret_cast<float2*>(p) = make_float2(a, b);
@@ -141,13 +159,15 @@ template <int B> __device__ __forceinline__ void sp_cp(uint32_t dst, const char*
 }
 
 template <class T, class TC, int MODE, bool TM>
-__global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
+__global__ void __launch_bounds__(SP_NT, (sp_minb<T, TC, TM>()))
     sweep_pair_kernel(const __grid_constant__ SpMaps maps, const SpArgs<T, TC> a) {
-    static_assert(sizeof(T) == sizeof(TC) && sizeof(T) >= 4, "FP64 or FP32 vectors with coefficients of the same type");
+    static_assert((std::is_same<T, TC>::value && sizeof(T) >= 4) ||
+                      (std::is_same<T, float>::value && std::is_same<TC, __nv_bfloat16>::value && TM),
+                  "FP64 or FP32 vectors with coefficients of the same type, or FP32 / BF16 with TMA staging");
     constexpr bool ZERO = (MODE & M_ZERO) != 0, PROL = (MODE & M_PROLONG) != 0, DOT = (MODE & M_DOT) != 0;
     static_assert((MODE & M_RESID) == 0, "the residual runs in a kernel of its own");
-    using G = SpGeom<T, TM>;
-    constexpr int ST = G::ST, W = G::W, HX = G::HX, NP = G::NP, TX = G::TX;
+    using G = SpGeom<T, TC, TM>;
+    constexpr int ST = G::ST, SC = G::SC, W = G::W, HX = G::HX, NP = G::NP, TX = G::TX;
     constexpr int QS = 32; // cells between the pairs of one lane (16 lanes x one pair each)
     extern __shared__ __align__(128) unsigned char sp_sm_raw[];
     // slots start on a 128-byte boundary of the shared window (TMA destinations)
@@ -160,6 +180,13 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
     // arrays in a coefficient slot, in elements
     constexpr int OB = (int)(G::OB / ST), OCX = (int)(G::OCX / ST), OCY = (int)(G::OCY / ST);
     constexpr int OCZ = (int)(G::OCZ / ST), OBX = (int)(G::OBX / ST), OBY = (int)(G::OBY / ST);
+    // the coefficient-typed arrays of slot s start at cof(s); their offsets in that type
+    // (the cp.async form, where the types agree, uses the offsets above from cs0)
+    constexpr int OCYc = (int)((G::OCY - G::OCX) / SC), OCZc = (int)((G::OCZ - G::OCX) / SC);
+    constexpr int OBXc = (int)((G::OBX - G::OCX) / SC), OBYc = (int)((G::OBY - G::OCX) / SC);
+    auto cof = [&](int sl) -> TC* {
+        return reinterpret_cast<TC*>(reinterpret_cast<unsigned char*>(cs0 + sl * CE) + G::OCX);
+    };
     const uint32_t xs0_u = (uint32_t)__cvta_generic_to_shared(xs0), cs0_u = (uint32_t)__cvta_generic_to_shared(cs0);
 
     const LevelOp<TC>& L = a.L;
@@ -240,21 +267,22 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
                     uint64_t* bar = &sp_full[sxi];
                     unsigned bytes = 0;
                     if (dox) bytes += (unsigned)(SP_XR * W * ST);
-                    if (doc) bytes += (unsigned)((3 * SP_CR + SP_YR) * W * ST + (i0 == 0 ? G::BXN * ST : 0) +
-                                                 (j0 == 0 ? W * ST : 0));
+                    if (doc) bytes += (unsigned)(SP_CR * W * ST + (2 * SP_CR + SP_YR) * W * SC + (i0 == 0 ? G::BXN * SC : 0) +
+                                                 (j0 == 0 ? W * SC : 0));
                     mbar_expect_tx(bar, bytes);
                     if (dox) tma_load_3d(xs0 + sxi * XE, &maps.x, i0 - HX, j0 - 2, p, bar);
                     if (doc) {
                         T* C = cs0 + sci * CE;
-                        tma_load_3d(C + OB, &maps.b, i0 - HX, j0 - 1, q, bar);
-                        tma_load_3d(C + OCX, &maps.cx, i0 - HX, j0 - 1, q, bar);
-                        tma_load_3d(C + OCY, &maps.cy, i0 - HX, j0 - 2, q, bar);
+                        TC* Cc = cof(sci);
+                        tma_load_3d(C, &maps.b, i0 - HX, j0 - 1, q, bar);
+                        tma_load_3d(Cc, &maps.cx, i0 - HX, j0 - 1, q, bar);
+                        tma_load_3d(Cc + OCYc, &maps.cy, i0 - HX, j0 - 2, q, bar);
                         if (q == -1) // the -z faces of plane 0 stand in for plane -1's +z faces
-                            tma_load_2d(C + OCZ, &maps.bzm, i0 - HX, j0 - 1, bar);
+                            tma_load_2d(Cc + OCZc, &maps.bzm, i0 - HX, j0 - 1, bar);
                         else
-                            tma_load_3d(C + OCZ, &maps.cz, i0 - HX, j0 - 1, q, bar);
-                        if (i0 == 0) tma_load_2d(C + OBX, &maps.bxm, j0 - G::BXS, q, bar);
-                        if (j0 == 0) tma_load_2d(C + OBY, &maps.bym, i0 - HX, q, bar);
+                            tma_load_3d(Cc + OCZc, &maps.cz, i0 - HX, j0 - 1, q, bar);
+                        if (i0 == 0) tma_load_2d(Cc + OBXc, &maps.bxm, j0 - G::BXS, q, bar);
+                        if (j0 == 0) tma_load_2d(Cc + OBYc, &maps.bym, i0 - HX, q, bar);
                     }
                 }
             }
@@ -392,8 +420,8 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
                 gxy[q] = pin[q] ? (long long)pi + (long long)nx * wj : 0;
                 // the -x face of cell pi - 1 and the -y faces of the pair: from the boundary-face
                 // buffers where the TMA form stages them, else from the cx / cy slots
-                cxl_off[q] = (TM && i0 == 0 && pi == 0) ? OBX + (pj - j0 + G::BXS) : OCX + fc + QS * q - 1;
-                cyd_off[q] = (TM && j0 == 0 && pj == 0) ? OBY + (pi - i0 + HX) : OCY + fx + QS * q - W;
+                cxl_off[q] = (TM && i0 == 0 && pi == 0) ? OBXc + (pj - j0 + G::BXS) : fc + QS * q - 1;
+                cyd_off[q] = (TM && j0 == 0 && pj == 0) ? OBYc + (pi - i0 + HX) : OCYc + fx + QS * q - W;
             }
             auto issue = [&](int p) {
                 if constexpr (TM) {
@@ -428,7 +456,7 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
                 const P2<T> xp0 = take(0, fx + QS * q, corr(pin[q], pi, wj, P0)); // x(P0): own column only
                 const P2<T> xp1 = take(1, fx + QS * q, corr(pin[q], pi, wj, P0 + 1)); // x(P0 + 1), published
                 en[q] = corr(pin[q], pi, wj, P0 + 2); // correction of the pair in plane t + 1
-                czp1[q] = sp_ld2<TC>(cs0 + OCZ + fc + QS * q);
+                czp1[q] = sp_ldc<T, TC>(cof(0) + OCZc + fc + QS * q);
                 czp2[q] = P2<T>{(T)0, (T)0};
                 A[q] = O0 ? xp1.a : xp1.b;
                 B[q] = O0 ? xp0.b : xp0.a;
@@ -440,6 +468,7 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
                 constexpr int O = decltype(Oc)::value;
                 issue(t + SP_D);
                 const T* C = cs0 + sc0 * CE;
+                const TC* Cc = cof(sc0);
                 T* X0 = xs0 + sx0 * XE;
                 const T* X1 = xs0 + sxm * XE;
                 const int q_out = t - 1;
@@ -459,10 +488,10 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
                         xnO = xs0[sx1 * XE + f + O];
                     }
                     // ---- coefficients of plane t ----
-                    const P2<T> b2 = sp_ld2<T>(C + OB + g), cx2p = sp_ld2<TC>(C + OCX + g);
-                    const P2<T> cy2p = sp_ld2<TC>(C + OCY + f), cyd2 = sp_ld2<TC>(C + cyd_off[q]);
-                    const P2<T> cz2 = sp_ld2<TC>(C + OCZ + g);
-                    const T cxl = (T)C[cxl_off[q]];
+                    const P2<T> b2 = sp_ld2<T>(C + OB + g), cx2p = sp_ldc<T, TC>(Cc + g);
+                    const P2<T> cy2p = sp_ldc<T, TC>(Cc + OCYc + f), cyd2 = sp_ldc<T, TC>(Cc + cyd_off[q]);
+                    const P2<T> cz2 = sp_ldc<T, TC>(Cc + OCZc + g);
+                    const T cxl = sp_c1<T, TC>(Cc + cxl_off[q]);
                     // ---- red cell pi + O of plane t, from old black values ----
                     T red = (T)0;
                     {
@@ -570,8 +599,8 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
                 gxy2[q] = pin2[q] ? (long long)wi[q] + (long long)nx * wj2 : 0;
                 gcy2[q] = (wi[q] >= 0 && wcy2 >= 0) ? (long long)wi[q] + (long long)nx * wcy2 : 0;
                 cx_bnd[q] = pi == -2 && !L.per_x;
-                cxl_off[q] = (TM && i0 == 0 && pi == 0) ? OBX + (pj - j0 + G::BXS) : OCX + fc + QS * q - 1;
-                cyd_off[q] = (TM && j0 == 0 && pj == 0) ? OBY + (pi - i0 + HX) : OCY + fx + QS * q - W;
+                cxl_off[q] = (TM && i0 == 0 && pi == 0) ? OBXc + (pj - j0 + G::BXS) : fc + QS * q - 1;
+                cyd_off[q] = (TM && j0 == 0 && pj == 0) ? OBYc + (pi - i0 + HX) : OCYc + fx + QS * q - W;
             }
             auto issue = [&](int p) {
                 if constexpr (!TM) { // (one pair per lane: NP == 1 in this form)
@@ -637,7 +666,7 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
                 if (has2) (void)take(1, fx2 + QS * q, corr(pin2[q], wi[q], wj2, P0 + 1));
                 en[q] = corr(pin[q], wi[q], wj, P0 + 2);
                 en2[q] = has2 ? corr(pin2[q], wi[q], wj2, P0 + 2) : (T)0;
-                czp1[q] = sp_ld2<TC>(cs0 + OCZ + fc + QS * q);
+                czp1[q] = sp_ldc<T, TC>(cof(0) + OCZc + fc + QS * q);
             }
             for (int t = z0 - 1; t <= z1; ++t) {
                 if (!sync_step(t + 1, sx1)) {
@@ -647,6 +676,7 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
                 issue(t + SP_D);
                 const int o = (pj + t) & 1;
                 const T* C = cs0 + sc0 * CE;
+                const TC* Cc = cof(sc0);
                 T* X0 = xs0 + sx0 * XE;
 #pragma unroll
                 for (int q = 0; q < NP; ++q) {
@@ -658,10 +688,10 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TM>()))
                         en[q] = corr(pin[q], wi[q], wj, t + 2);
                         if (has2) en2[q] = corr(pin2[q], wi[q], wj2, t + 2);
                     }
-                    const P2<T> b2 = sp_ld2<T>(C + OB + g), cx2p = sp_ld2<TC>(C + OCX + g);
-                    const P2<T> cy2p = sp_ld2<TC>(C + OCY + f), cyd2 = sp_ld2<TC>(C + cyd_off[q]);
-                    const P2<T> cz2 = sp_ld2<TC>(C + OCZ + g);
-                    const T cxl = (T)C[cxl_off[q]];
+                    const P2<T> b2 = sp_ld2<T>(C + OB + g), cx2p = sp_ldc<T, TC>(Cc + g);
+                    const P2<T> cy2p = sp_ldc<T, TC>(Cc + OCYc + f), cyd2 = sp_ldc<T, TC>(Cc + cyd_off[q]);
+                    const P2<T> cz2 = sp_ldc<T, TC>(Cc + OCZc + g);
+                    const T cxl = sp_c1<T, TC>(Cc + cxl_off[q]);
                     if (role == 1 || o != side) { // a ring-column cell is relaxed where it is red
                         T xout = (T)0, xsv = (T)0, xnv = (T)0;
                         if constexpr (!ZERO || PROL) {

@@ -206,8 +206,13 @@ static void launch_pair_sweep_tm(cudaStream_t s, dim3 grid, int mode, const SpMa
 }
 template <class T, class TC>
 static void launch_pair_sweep(cudaStream_t s, dim3 grid, int mode, bool tm, const SpMaps& m, const SpArgs<T, TC>& a) {
-    if (tm) launch_pair_sweep_tm<T, TC, true>(s, grid, mode, m, a);
-    else launch_pair_sweep_tm<T, TC, false>(s, grid, mode, m, a);
+    if constexpr (!std::is_same<T, TC>::value) { // BF16 coefficients: TMA staging only
+        if (!tm) throw Error(MF3D_E_INVALID, "x-pair sweep with BF16 coefficients needs TMA staging");
+        launch_pair_sweep_tm<T, TC, true>(s, grid, mode, m, a);
+    } else {
+        if (tm) launch_pair_sweep_tm<T, TC, true>(s, grid, mode, m, a);
+        else launch_pair_sweep_tm<T, TC, false>(s, grid, mode, m, a);
+    }
 }
 // dynamic shared memory and resident CTAs per SM of one x-pair sweep variant
 template <class T, class TC, int MODE, bool TM> static int pair_sweep_setup() {
@@ -396,15 +401,16 @@ template <class E> static CUtensorMap make_map2(const void* base, int d0, int d1
 // Whether the x-pair sweep stages a level by TMA: no periodic axis, and rows of the arrays
 // and of the boundary-face planes that are whole multiples of 16 bytes (a box row of
 // cp.async.bulk.tensor starts on a 16-byte boundary).
-template <class T> static bool sp_tma_ok(const Geom& g, const mf3d_bc& bc) {
+template <class T, class TC = T> static bool sp_tma_ok(const Geom& g, const mf3d_bc& bc) {
     if (bc.type[0] == MF3D_BC_PERIODIC || bc.type[2] == MF3D_BC_PERIODIC || bc.type[4] == MF3D_BC_PERIODIC)
         return false;
-    return g.nx % 2 == 0 && ((size_t)g.nx * sizeof(T)) % 16 == 0 && ((size_t)g.ny * sizeof(T)) % 16 == 0;
+    return g.nx % 2 == 0 && ((size_t)g.nx * sizeof(T)) % 16 == 0 && ((size_t)g.ny * sizeof(T)) % 16 == 0 &&
+           ((size_t)g.nx * sizeof(TC)) % 16 == 0 && ((size_t)g.ny * sizeof(TC)) % 16 == 0;
 }
 // Tensor maps of the TMA-staged x-pair sweep of one level (x: the sweep's input buffer).
 template <class T, class TC>
 static SpMaps make_sp_maps(const Geom& g, const T* x, const T* b, const LevelOp<TC>& op) {
-    using G = SpGeom<T, true>;
+    using G = SpGeom<T, TC, true>;
     SpMaps m;
     m.x = make_map<T>(x, g, G::W, SP_XR);
     m.b = make_map<T>(b, g, G::W, SP_CR);
@@ -570,6 +576,10 @@ static void launch_coarse(cudaStream_t s, const CoarsePlan& p, const CoarseArgs&
 }
 
 template <class T, class TC> class VCycle : public VCycleBase {
+    // the x-pair sweep serves FP64 / FP64, FP32 / FP32 and FP32 / BF16 (vector / coefficient)
+    static constexpr bool kPair = sizeof(T) == sizeof(TC) ||
+                                  (std::is_same<T, float>::value && std::is_same<TC, __nv_bfloat16>::value);
+
   public:
     // b0: level-0 right-hand side in the V-cycle's type (the PCG residual or its FP32 copy);
     // r64: the FP64 residual (dot products, and the right-hand side when the whole V-cycle is
@@ -648,21 +658,22 @@ template <class T, class TC> class VCycle : public VCycleBase {
         if (n_tma_) set_tma_smem();
         // levels the x-pair sweep serves (single solves, every mode but the fused residual):
         // the FP64 V-cycle wherever nx is even and a periodic axis is a whole number of tiles
-        // (TMA staging where the grid allows it, cp.async otherwise); the FP32 V-cycle where TMA
-        // staging applies (else the quad sweep); BF16 coefficients keep the quad sweep
+        // (TMA staging where the grid allows it, cp.async otherwise); the FP32 V-cycle, with FP32
+        // or BF16 coefficients, where TMA staging applies (else the quad sweep)
         pair_.assign(Lt, 0);
         pair_tm_.assign(Lt, 0);
         pmaps_.resize(Lt);
-        if constexpr (sizeof(T) == sizeof(TC)) {
+        if constexpr (kPair) {
             for (int l = 0; l < Lt; ++l) {
                 const Geom& g = G[l];
                 if (g.nx % 2) continue;
                 if (bc.type[0] == MF3D_BC_PERIODIC && g.nx % SP_TX) continue;
                 if (bc.type[2] == MF3D_BC_PERIODIC && g.ny % SP_TY) continue;
-                if (sizeof(T) == 4 && !sp_tma_ok<T>(g, bc)) continue;
+                const bool tm = allow_tma && sp_tma_ok<T, TC>(g, bc);
+                if (sizeof(T) == 4 && !tm) continue;
                 pair_[l] = 1;
                 ++n_pair_;
-                if (sp_tma_ok<T>(g, bc)) { // TMA staging; maps for both x buffers
+                if (tm) { // TMA staging; maps for both x buffers
                     const T* b = l == 0 ? b0_ : (const T*)bl_[l]->p;
                     pmaps_[l][0] = make_sp_maps<T, TC>(g, (const T*)xa_[l]->p, b, ops_[l]);
                     pmaps_[l][1] = make_sp_maps<T, TC>(g, (const T*)xb_[l]->p, b, ops_[l]);
@@ -1022,7 +1033,7 @@ template <class T, class TC> class VCycle : public VCycleBase {
             rec_->push_back(r);
             return;
         }
-        if constexpr (sizeof(T) == sizeof(TC)) {
+        if constexpr (kPair) {
             if (pair_[l] && !(mode & M_RESID)) {
                 pair_sweep(s, l, x_in, x_out, e, mode, dot_out);
                 return;
@@ -1084,8 +1095,8 @@ template <class T, class TC> class VCycle : public VCycleBase {
 
     // ---- the x-pair sweep (kernels_sweep_pair.cuh) ----
     template <int MODE> void set_pair_one() {
-        if constexpr (sizeof(T) == sizeof(TC)) {
-            pocc_[MODE & 15] = pair_sweep_setup<T, TC, MODE, false>();
+        if constexpr (kPair) {
+            if constexpr (std::is_same<T, TC>::value) pocc_[MODE & 15] = pair_sweep_setup<T, TC, MODE, false>();
             pocc_tm_[MODE & 15] = pair_sweep_setup<T, TC, MODE, true>();
         }
     }
@@ -1100,7 +1111,7 @@ template <class T, class TC> class VCycle : public VCycleBase {
         set_pair_one<M_ZERO | M_PROLONG | M_DOT>();
     }
     void pair_sweep(cudaStream_t s, int l, const T* x_in, T* x_out, const T* e, int mode, double* dot_out) {
-        if constexpr (sizeof(T) == sizeof(TC)) {
+        if constexpr (kPair) {
             const Geom& g = G_[l];
             SpArgs<T, TC> a{};
             a.L = ops_[l];
@@ -1119,7 +1130,7 @@ template <class T, class TC> class VCycle : public VCycleBase {
             a.err = scr_.err;
             const bool tm = pair_tm_[l] != 0;
             const long long resident = (long long)std::max(1, (tm ? pocc_tm_ : pocc_)[mode & 15]) * num_sms();
-            const dim3 grid = pair_grid(g, resident, &a.zchunk, tm ? sp_tx<T, true>() : sp_tx<T, false>());
+            const dim3 grid = pair_grid(g, resident, &a.zchunk, tm ? sp_tx<T, TC, true>() : sp_tx<T, TC, false>());
             if ((mode & M_DOT) && grid.x > scr_.partial_cap) throw Error(MF3D_E_INVALID, "reduction scratch too small");
             static const SpMaps no_maps{};
             const SpMaps& m = !tm ? no_maps : pmaps_[l][x_in == (const T*)xb_[l]->p ? 1 : 0];
@@ -1174,7 +1185,7 @@ template <class T, class TC> class VCycle : public VCycleBase {
     void resid_restrict(cudaStream_t s, int l, const T* x, T* out) {
         const Geom& g = G_[l];
         const T* b = l == 0 ? b0_ : (const T*)bl_[l]->p;
-        if constexpr (sizeof(TC) >= 4) { // staged: 32 x 16 tiles of x-pairs, even z chunks
+        if constexpr (sizeof(TC) >= 4 || kPair) { // staged: 32 x 16 tiles of x-pairs, even z chunks
             const int gx = (g.nx + RR_TX - 1) / RR_TX, gy = (g.ny + RR_TY - 1) / RR_TY, ncz = g.nz / 2;
             const long long tiles = (long long)gx * gy;
             const int nzc = (int)std::max<long long>(
@@ -1216,12 +1227,11 @@ template <class T, class TC> class VCycle : public VCycleBase {
     std::vector<int> tma_;
     std::vector<std::array<Maps4, 2>> maps_;
     int n_tma_ = 0;
-    // Staged levels with FP32 or FP64 coefficients: the residual and its restriction in a
-    // kernel of their own (resid_restrict_staged_kernel) after the last pre-sweep, which
-    // computes every cell's residual exactly and is faster than the fused RESID sweep
-    // (measured at 256^3 in FP32: 0.152 + 0.069 ms against 0.280 ms).  BF16 coefficients keep
-    // the fused sweep (cp.async moves at least 4 bytes).
-    static constexpr bool split_resid_ = sizeof(TC) >= 4;
+    // Staged levels: the residual and its restriction in a kernel of their own
+    // (resid_restrict_staged_kernel) after the last pre-sweep, which computes every cell's
+    // residual exactly and is faster than the fused RESID sweep (measured at 256^3 in FP32:
+    // 0.152 + 0.069 ms against 0.280 ms).  Batched solves keep the fused sweep.
+    static constexpr bool split_resid_ = sizeof(TC) >= 4 || kPair;
     int occ_[16] = {}; // resident staged-sweep CTAs per SM, by mode
     std::vector<int> pair_;    // levels served by the x-pair sweep
     std::vector<int> pair_tm_; // ... with TMA staging
@@ -2145,7 +2155,7 @@ int mf3d_gsrb(const mf3d_grid* g, const mf3d_bc* bc, int pin, const double* K, c
             a.b = b;
             a.err = err.as<int>();
             const dim3 grid = pair_grid(L.G, (long long)std::max(1, occ) * num_sms(), &a.zchunk,
-                                        tm ? sp_tx<double, true>() : sp_tx<double, false>());
+                                        tm ? sp_tx<double, double, true>() : sp_tx<double, double, false>());
             SpMaps maps[2] = {};
             if (tm)
                 for (int q = 0; q < 2; ++q) maps[q] = make_sp_maps<double, double>(L.G, pbufs[q], b, L.op);

@@ -208,6 +208,34 @@ def test_cluster_coarse_end_matches_one_cta_tail(mf3d, monkeypatch, shape, level
     assert _rel(z["cluster"], z["tail"]) < (1e-12 if prec == "fp64" else 1e-5)
 
 
+@pytest.mark.parametrize("shape,levels", [((64, 64, 64), 5), ((32, 48, 64), 4), ((16, 16, 128), 3)])
+@pytest.mark.parametrize("bcname", ["darcy", "all_dirichlet"])
+def test_bf16_vcycle_staged_matches_unstaged(mf3d, monkeypatch, shape, levels, bcname):
+    """The BF16-coefficient V-cycle on the TMA-staged x-pair sweep and the staged residual +
+    restriction against the same V-cycle on the unstaged sweep (MF3D_NO_TMA): the same BF16
+    coefficients and FP32 arithmetic, so equal to FP32 rounding (1e-5 of the max)."""
+    M = mf3d
+    rng = np.random.default_rng(zlib.crc32(repr((shape, levels, bcname, "bf16")).encode()))
+    K = np.exp(rng.normal(size=shape))
+    r = rng.normal(size=shape)
+    g = M.Grid3D(shape[2], shape[1], shape[0], 1.0)
+    case = [c for c in BC_CASES if c[0] == bcname][0]
+    bc = _bcs(M, case[1], case[2])
+    cfg = M.HeadSolveConfig(mg_levels=levels, precision=M.PREC_BF16)
+    z = {}
+    for mode in ("staged", "unstaged"):
+        if mode == "unstaged":
+            monkeypatch.setenv("MF3D_NO_TMA", "1")
+        s = M.HeadSolver(g, bc, cfg)
+        s.set_K(_t(K))
+        zz = _t(np.zeros(shape))
+        s.vcycle(_t(r), zz)
+        z[mode] = _np(zz)
+        s.close()
+        monkeypatch.delenv("MF3D_NO_TMA", raising=False)
+    assert _rel(z["staged"], z["unstaged"]) < 1e-5
+
+
 def _lognormal(shape, sigma, seed):
     return np.exp(sigma * np.random.default_rng(seed).normal(size=shape))
 
