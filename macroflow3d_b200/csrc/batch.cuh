@@ -36,6 +36,19 @@ template <class T, class TC, int MODE> static int tma_batch_setup() {
     return n;
 }
 
+// dynamic shared memory and resident CTAs per SM of a batched x-pair sweep (TMA form)
+template <class T, class TC, int MODE> static int pair_batch_setup() {
+    const size_t smem = sp_smem_bytes<T, TC, true>();
+    MF3D_CK(cudaFuncSetAttribute(sweep_pair_kernel<T, TC, MODE, true, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    MF3D_CK(cudaFuncSetAttribute(sweep_pair_kernel<T, TC, MODE, true, true>,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
+    int n = 0;
+    MF3D_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_pair_kernel<T, TC, MODE, true, true>, SP_NT, smem));
+    if (n < 1) throw Error(MF3D_E_CUDA, "x-pair sweep does not fit on an SM");
+    return n;
+}
+
 class BatchSolverBase {
   public:
     virtual ~BatchSolverBase() {}
@@ -66,8 +79,10 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
     using VC = VCycle<T, TC>;
     using Rec = typename VC::RecSweep;
 
-    // one batched launch of a sweep position: staged (TMA) or L1 form
+    // one batched launch of a sweep position: x-pair (TMA), staged quad (TMA) or L1 form
     struct Launch {
+        bool pair = false;
+        SpArgs<T, TC> pa0{}; // x-pair: the launch-wide argument
         bool tma = false;
         int nseg = 0, total = 0;
         unsigned grid = 0;
@@ -82,7 +97,9 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
         int phase, level, sw, mode;
         std::vector<int> real; // realisation of each record
         std::vector<Rec> rec;
-        int path = 0, chunks = 1; // 0: staged where aligned, 1: L1 only; z chunks per tile
+        // 0: staged quad where aligned, 1: L1 only, 2: x-pair where it serves (else as 0);
+        // z chunks per tile
+        int path = 0, chunks = 1;
         std::vector<Launch> launches;
     };
 
@@ -101,6 +118,16 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
         occ_[M_ZERO | M_DOT] = tma_batch_setup<T, TC, M_ZERO | M_DOT>();
         occ_[M_PROLONG | M_DOT] = tma_batch_setup<T, TC, M_PROLONG | M_DOT>();
         occ_[M_ZERO | M_PROLONG | M_DOT] = tma_batch_setup<T, TC, M_ZERO | M_PROLONG | M_DOT>();
+        if constexpr (VC::kPair) {
+            pocc_[0] = pair_batch_setup<T, TC, 0>();
+            pocc_[M_ZERO] = pair_batch_setup<T, TC, M_ZERO>();
+            pocc_[M_PROLONG] = pair_batch_setup<T, TC, M_PROLONG>();
+            pocc_[M_ZERO | M_PROLONG] = pair_batch_setup<T, TC, M_ZERO | M_PROLONG>();
+            pocc_[M_DOT] = pair_batch_setup<T, TC, M_DOT>();
+            pocc_[M_ZERO | M_DOT] = pair_batch_setup<T, TC, M_ZERO | M_DOT>();
+            pocc_[M_PROLONG | M_DOT] = pair_batch_setup<T, TC, M_PROLONG | M_DOT>();
+            pocc_[M_ZERO | M_PROLONG | M_DOT] = pair_batch_setup<T, TC, M_ZERO | M_PROLONG | M_DOT>();
+        }
 
         // ---- record every realisation's V-cycle ----
         std::vector<std::vector<Rec>> recs(R);
@@ -337,13 +364,14 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
             t.ms_default = time_launches(o.mode, o.launches, reps);
             int best_path = o.path, best_chunks = o.chunks;
             double best = t.ms_default;
-            bool any_tma = false;
+            bool any_tma = false, any_pair = false;
             int nzmin = 1 << 30;
             for (const Rec& x : o.rec) {
                 any_tma |= x.tma;
+                any_pair |= x.pair;
                 nzmin = std::min(nzmin, x.g.nz);
             }
-            for (int path = any_tma ? 0 : 1; path < 2; ++path)
+            for (int path = any_tma ? 0 : 1; path < (any_pair ? 3 : 2); ++path)
                 for (int chunks = 1; chunks <= 8 && (chunks == 1 || 2 * chunks <= nzmin); chunks *= 2) {
                     if (path == o.path && chunks == o.chunks) continue;
                     std::vector<Launch> cand = build(o, path, chunks);
@@ -375,16 +403,21 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
 
   private:
     void default_choice(Op& o) {
-        bool any_tma = false;
-        long long tiles = 0, cols = 0;
+        bool any_tma = false, any_pair = false;
+        long long tiles = 0, cols = 0, ptiles = 0;
         for (const Rec& x : o.rec) {
             any_tma |= x.tma;
+            any_pair |= x.pair;
             const int TX = TmaSweepCfg<T, TC, 0>::TX, TY = TmaSweepCfg<T, TC, 0>::TY;
             if (x.tma) tiles += (long long)((x.g.nx + TX - 1) / TX) * ((x.g.ny + TY - 1) / TY);
+            if (x.pair) ptiles += (long long)((x.g.nx + pair_tx() - 1) / pair_tx()) * ((x.g.ny + SP_TY - 1) / SP_TY);
             cols += (long long)((x.g.nx + SW_TX - 1) / SW_TX) * ((x.g.ny + SW_TY - 1) / SW_TY);
         }
-        o.path = any_tma ? 0 : 1;
-        if (o.path == 0) {
+        o.path = any_pair ? 2 : (any_tma ? 0 : 1);
+        if (o.path == 2) {
+            const long long resident = (long long)std::max(1, pocc_[o.mode & 15]) * num_sms();
+            o.chunks = (int)std::max<long long>(1, std::min<long long>(8, resident / std::max(1LL, ptiles)));
+        } else if (o.path == 0) {
             const long long resident = (long long)std::max(1, occ_[o.mode & 15]) * num_sms();
             o.chunks = (int)std::max<long long>(1, std::min<long long>(8, resident / std::max(1LL, tiles)));
         } else {
@@ -399,10 +432,54 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
 
     // the launches of sweep position o for a choice: the staged sweep for the realisations
     // whose level has a staged form (path 0), the L1 sweep for the others
+    static constexpr int pair_tx() { return sp_tx<T, TC, true>(); }
+
     std::vector<Launch> build(const Op& o, int path, int chunks) const {
-        std::vector<int> ts, ls;
-        for (int i = 0; i < (int)o.rec.size(); ++i) (path == 0 && o.rec[i].tma ? ts : ls).push_back(i);
+        std::vector<int> ps, ts, ls;
+        for (int i = 0; i < (int)o.rec.size(); ++i) {
+            const Rec& x = o.rec[i];
+            if (path == 2 && x.pair) ps.push_back(i);
+            else if (path != 1 && x.tma) ts.push_back(i);
+            else ls.push_back(i);
+        }
         std::vector<Launch> out;
+        if (!ps.empty()) {
+            std::vector<int> off(1, 0);
+            std::vector<SpArgs<T, TC>> args;
+            std::vector<SpMaps> maps;
+            for (int i : ps) {
+                const Rec& x = o.rec[i];
+                HeadSolver& H = *hs_[o.real[i]];
+                SpArgs<T, TC> a = x.pa;
+                a.zchunk = chunk_planes(x.g.nz, chunks);
+                a.stop = &H.state_.as<PcgState>()->stop;
+                const int ntiles = ((x.g.nx + pair_tx() - 1) / pair_tx()) * ((x.g.ny + SP_TY - 1) / SP_TY);
+                const int items = ntiles * ((x.g.nz + a.zchunk - 1) / a.zchunk);
+                if ((o.mode & M_DOT) && (size_t)items > vc_of(o.real[i])->scratch().partial_cap)
+                    throw Error(MF3D_E_INVALID, "reduction scratch too small");
+                off.push_back(off.back() + items);
+                args.push_back(a);
+                maps.push_back(*x.pmaps);
+            }
+            Blob b;
+            const size_t oo = b.add(off.data(), off.size() * sizeof(int));
+            const size_t oa = b.add(args.data(), args.size() * sizeof(args[0]));
+            const size_t om = b.add(maps.data(), maps.size() * sizeof(SpMaps));
+            Launch L;
+            L.pair = true;
+            L.nseg = (int)ps.size();
+            L.total = off.back();
+            L.mem = b.upload();
+            unsigned char* base = L.mem->template as<unsigned char>();
+            L.pa0.seg_off = reinterpret_cast<const int*>(base + oo);
+            L.pa0.seg_args = reinterpret_cast<const SpArgs<T, TC>*>(base + oa);
+            L.pa0.seg_maps = reinterpret_cast<const SpMaps*>(base + om);
+            L.pa0.nseg = L.nseg;
+            L.pa0.total = L.total;
+            const long long resident = (long long)std::max(1, pocc_[o.mode & 15]) * num_sms();
+            L.grid = (unsigned)std::max<long long>(1, std::min<long long>(L.total, resident));
+            out.push_back(std::move(L));
+        }
         if (!ts.empty()) {
             const int TX = TmaSweepCfg<T, TC, 0>::TX, TY = TmaSweepCfg<T, TC, 0>::TY;
             std::vector<int> off(1, 0);
@@ -481,7 +558,14 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
     VC* vc_of(int r) const { return static_cast<VC*>(hs_[r]->vc_.get()); }
 
     template <int MODE> void launch_one(cudaStream_t s, const Launch& L) const {
-        if (L.tma) {
+        if (L.pair) {
+            if constexpr (VC::kPair && (MODE & M_RESID) == 0) {
+                sweep_pair_kernel<T, TC, MODE, true, true>
+                    <<<L.grid, SP_NT, sp_smem_bytes<T, TC, true>(), s>>>(SpMaps{}, L.pa0);
+            } else {
+                throw Error(MF3D_E_INVALID, "x-pair sweep: unsupported batched mode");
+            }
+        } else if (L.tma) {
             using C = TmaSweepCfg<T, TC, MODE>;
             sweep_tma_kernel<T, TC, MODE, true><<<L.grid, C::NT, C::SMEM, s>>>(TmaMaps{}, L.a0);
         } else {
@@ -636,6 +720,7 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
     cudaStream_t s_ = nullptr, own_stream_ = nullptr;
     bool flexible_ = false;
     int occ_[16] = {};
+    int pocc_[16] = {}; // resident batched x-pair-sweep CTAs per SM, by mode
     std::vector<Op> ops_;
     std::unique_ptr<DevMem> tail_mem_, pcg_mem_;
     size_t tail_smem_ = 0;

@@ -93,6 +93,7 @@ template <class T, class TC, bool TM> constexpr int sp_minb() {
     return (sizeof(T) == 8 || SpGeom<T, TC, TM>::NP == 2) ? 2 : 3;
 }
 
+struct SpMaps;
 template <class T, class TC> struct SpArgs {
     LevelOp<TC> L;
     const T* x_in; // ignored with M_ZERO
@@ -106,6 +107,14 @@ template <class T, class TC> struct SpArgs {
     double* dot_out;
     int zchunk; // planes per work item
     int* err;   // set to 1 when a staging wait gives up (TMA form)
+    const int* stop; // batched launches: the realisation's stop flag (its items are skipped)
+    // batched launches, the launch-wide argument only: work items [seg_off[s], seg_off[s+1])
+    // belong to realisation segment s, whose arguments and tensor maps are seg_args[s] and
+    // seg_maps[s] (device memory, 64-byte aligned)
+    const int* seg_off;
+    const SpArgs* seg_args;
+    const SpMaps* seg_maps;
+    int nseg, total;
 };
 
 // Tensor maps of the TMA form: x / b / cx / cz / cy boxes of W x (XR | CR | CR | CR | YR) x 1;
@@ -158,9 +167,12 @@ template <int B> __device__ __forceinline__ void sp_cp(uint32_t dst, const char*
                      : "memory");
 }
 
-template <class T, class TC, int MODE, bool TM>
+// BATCH: one launch sweeps the same level depth of several realisations (TMA form); the
+// CTAs walk the concatenated (tile, z chunk) items of every realisation whose solve is running.
+template <class T, class TC, int MODE, bool TM, bool BATCH = false>
 __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TC, TM>()))
-    sweep_pair_kernel(const __grid_constant__ SpMaps maps, const SpArgs<T, TC> a) {
+    sweep_pair_kernel(const __grid_constant__ SpMaps maps0, const SpArgs<T, TC> a0) {
+    static_assert(!BATCH || TM, "batched launches use the TMA form");
     static_assert((std::is_same<T, TC>::value && sizeof(T) >= 4) ||
                       (std::is_same<T, float>::value && std::is_same<TC, __nv_bfloat16>::value && TM),
                   "FP64 or FP32 vectors with coefficients of the same type, or FP32 / BF16 with TMA staging");
@@ -189,13 +201,11 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TC, TM>()))
     };
     const uint32_t xs0_u = (uint32_t)__cvta_generic_to_shared(xs0), cs0_u = (uint32_t)__cvta_generic_to_shared(cs0);
 
-    const LevelOp<TC>& L = a.L;
-    const int nx = L.nx, ny = L.ny, nz = L.nz;
-    const size_t nxy = (size_t)nx * ny;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int ntx = (nx + TX - 1) / TX, ntiles = ntx * ((ny + SP_TY - 1) / SP_TY);
-    const int total = ntiles * ((nz + a.zchunk - 1) / a.zchunk);
-    const T dx2 = (T)L.dx2;
+    // work items of the launch: one realisation's, or (BATCH) every segment's
+    const int gtotal = BATCH ? a0.total
+                             : ((a0.L.nx + TX - 1) / TX) * ((a0.L.ny + SP_TY - 1) / SP_TY) *
+                                   ((a0.L.nz + a0.zchunk - 1) / a0.zchunk);
     auto divide = [](T num, T den) -> T {
         if constexpr (sizeof(T) == 4) return __fdividef(num, den); // preconditioner: 2-ulp division
         else return num / den;
@@ -218,9 +228,34 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TC, TM>()))
         }
     }
 
-    for (int item = blockIdx.x; item < total && !fail; item += gridDim.x) {
+    for (int gitem = blockIdx.x; gitem < gtotal && !fail; gitem += gridDim.x) {
+        int sg = 0, item = gitem, nitems = gtotal; // segment, item within it, its item count
+        if constexpr (BATCH) {
+            sg = find_seg(a0.seg_off, a0.nseg, gitem);
+            const int o = __ldg(a0.seg_off + sg);
+            item = gitem - o;
+            nitems = __ldg(a0.seg_off + sg + 1) - o;
+        }
+        const SpArgs<T, TC>& a = BATCH ? a0.seg_args[sg] : a0;
+        const SpMaps& maps = BATCH ? a0.seg_maps[sg] : maps0;
+        if constexpr (BATCH) {
+            if (a.stop && *a.stop) continue; // that realisation's solve has finished (CTA-uniform)
+        }
+        const LevelOp<TC>& L = a.L;
+        const int nx = L.nx, ny = L.ny, nz = L.nz;
+        const size_t nxy = (size_t)nx * ny;
+        const int ntx = (nx + TX - 1) / TX, ntiles = ntx * ((ny + SP_TY - 1) / SP_TY);
+        const T dx2 = (T)L.dx2;
         if constexpr (TM) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads(); // the previous item's reads (and generic writes) of the slots are done
+        if constexpr (BATCH) {
+            if (tid == 0) { // tensor maps read from global memory: order them before their use
+                const CUtensorMap* mp[8] = {&maps.x, &maps.b, &maps.cx, &maps.cy, &maps.cz, &maps.bxm, &maps.bym, &maps.bzm};
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(mp[k]) : "memory");
+            }
+        }
         const int tile = item % ntiles;
         const int z0 = (item / ntiles) * a.zchunk, z1 = min(z0 + a.zchunk, nz);
         const int i0 = (tile % ntx) * TX, j0 = (tile / ntx) * SP_TY;
@@ -719,10 +754,34 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TC, TM>()))
             }
         }
         if constexpr (!TM) asm volatile("cp.async.wait_all;" ::: "memory");
+        if constexpr (BATCH && DOT) {
+            // this item's share of <r64, x_out>; the last item of the realisation adds the
+            // items' partials in index order (deterministic)
+            __shared__ double sp_red[SP_NT / 32];
+            double v = dot_acc;
+            dot_acc = 0.0;
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) sp_red[warp] = v;
+            __syncthreads();
+            if (tid == 0 && !fail) {
+                double sum = 0.0;
+                for (int w = 0; w < SP_NT / 32; ++w) sum += sp_red[w];
+                a.dot_partials[item] = sum;
+                __threadfence();
+                if (atomicAdd(a.dot_ticket, 1u) == (unsigned)nitems - 1) {
+                    __threadfence();
+                    double acc = 0.0;
+                    for (int i = 0; i < nitems; ++i) acc += __ldcg(a.dot_partials + i);
+                    *a.dot_out = acc;
+                    *a.dot_ticket = 0u;
+                }
+            }
+            __syncthreads();
+        }
     }
-    if constexpr (DOT) {
+    if constexpr (DOT && !BATCH) {
         double v[1] = {dot_acc}, out[1];
-        if (grid_sums<SP_NT, 1>(v, a.dot_partials, a.dot_ticket, gridDim.x, out)) *a.dot_out = out[0];
+        if (grid_sums<SP_NT, 1>(v, a0.dot_partials, a0.dot_ticket, gridDim.x, out)) *a0.dot_out = out[0];
     }
 }
 

@@ -576,11 +576,11 @@ static void launch_coarse(cudaStream_t s, const CoarsePlan& p, const CoarseArgs&
 }
 
 template <class T, class TC> class VCycle : public VCycleBase {
+  public:
     // the x-pair sweep serves FP64 / FP64, FP32 / FP32 and FP32 / BF16 (vector / coefficient)
     static constexpr bool kPair = sizeof(T) == sizeof(TC) ||
                                   (std::is_same<T, float>::value && std::is_same<TC, __nv_bfloat16>::value);
 
-  public:
     // b0: level-0 right-hand side in the V-cycle's type (the PCG residual or its FP32 copy);
     // r64: the FP64 residual (dot products, and the right-hand side when the whole V-cycle is
     // the coarse tail).
@@ -760,6 +760,9 @@ template <class T, class TC> class VCycle : public VCycleBase {
         const TmaMaps* maps;
         SweepArgs<T, TC, T> la; // L1 form, z chunk unset
         Geom g;
+        bool pair;            // the x-pair sweep's TMA form serves this sweep
+        SpArgs<T, TC> pa;     // its arguments, z chunk unset
+        const SpMaps* pmaps;  // its tensor maps
     };
     struct RecTail {
         Tail2Args a;
@@ -1030,6 +1033,15 @@ template <class T, class TC> class VCycle : public VCycleBase {
             r.tma = tma;
             if (tma) r.ta = tma_args(l, x_in, x_out, e, b_coarse, mode, dot_out, &r.maps);
             r.la = ldg_args(l, x_in, x_out, e, b_coarse, dot_out);
+            r.pair = false;
+            r.pmaps = nullptr;
+            if constexpr (kPair) {
+                if (pair_[l] && pair_tm_[l] && !(mode & M_RESID)) {
+                    r.pair = true;
+                    r.pa = pair_args(l, x_in, x_out, e, dot_out);
+                    r.pmaps = &pair_maps(l, x_in, mode);
+                }
+            }
             rec_->push_back(r);
             return;
         }
@@ -1110,32 +1122,41 @@ template <class T, class TC> class VCycle : public VCycleBase {
         set_pair_one<M_PROLONG | M_DOT>();
         set_pair_one<M_ZERO | M_PROLONG | M_DOT>();
     }
+    // arguments of the x-pair sweep of level l, but for its z chunk
+    SpArgs<T, TC> pair_args(int l, const T* x_in, T* x_out, const T* e, double* dot_out) const {
+        SpArgs<T, TC> a{};
+        a.L = ops_[l];
+        a.x_in = x_in;
+        a.b = l == 0 ? b0_ : (const T*)bl_[l]->p;
+        a.x_out = x_out;
+        a.e_c = e;
+        if (l + 1 < (int)G_.size()) {
+            a.ncx = G_[l + 1].nx;
+            a.ncy = G_[l + 1].ny;
+        }
+        a.r64 = r64_;
+        a.dot_partials = scr_.partials;
+        a.dot_ticket = scr_.tickets + 0;
+        a.dot_out = dot_out;
+        a.err = scr_.err;
+        return a;
+    }
+    // tensor maps of the TMA form of level l for the input buffer x_in
+    const SpMaps& pair_maps(int l, const T* x_in, int mode) const {
+        if (!(mode & M_ZERO) && x_in != (const T*)xa_[l]->p && x_in != (const T*)xb_[l]->p)
+            throw Error(MF3D_E_INVALID, "sweep input is not a level buffer");
+        return pmaps_[l][x_in == (const T*)xb_[l]->p ? 1 : 0];
+    }
     void pair_sweep(cudaStream_t s, int l, const T* x_in, T* x_out, const T* e, int mode, double* dot_out) {
         if constexpr (kPair) {
             const Geom& g = G_[l];
-            SpArgs<T, TC> a{};
-            a.L = ops_[l];
-            a.x_in = x_in;
-            a.b = l == 0 ? b0_ : (const T*)bl_[l]->p;
-            a.x_out = x_out;
-            a.e_c = e;
-            if (l + 1 < (int)G_.size()) {
-                a.ncx = G_[l + 1].nx;
-                a.ncy = G_[l + 1].ny;
-            }
-            a.r64 = r64_;
-            a.dot_partials = scr_.partials;
-            a.dot_ticket = scr_.tickets + 0;
-            a.dot_out = dot_out;
-            a.err = scr_.err;
+            SpArgs<T, TC> a = pair_args(l, x_in, x_out, e, dot_out);
             const bool tm = pair_tm_[l] != 0;
             const long long resident = (long long)std::max(1, (tm ? pocc_tm_ : pocc_)[mode & 15]) * num_sms();
             const dim3 grid = pair_grid(g, resident, &a.zchunk, tm ? sp_tx<T, TC, true>() : sp_tx<T, TC, false>());
             if ((mode & M_DOT) && grid.x > scr_.partial_cap) throw Error(MF3D_E_INVALID, "reduction scratch too small");
             static const SpMaps no_maps{};
-            const SpMaps& m = !tm ? no_maps : pmaps_[l][x_in == (const T*)xb_[l]->p ? 1 : 0];
-            if (tm && !(mode & M_ZERO) && x_in != (const T*)xa_[l]->p && x_in != (const T*)xb_[l]->p)
-                throw Error(MF3D_E_INVALID, "sweep input is not a level buffer");
+            const SpMaps& m = !tm ? no_maps : pair_maps(l, x_in, mode);
             launch_pair_sweep<T, TC>(s, grid, mode, tm, m, a);
         }
     }
