@@ -54,6 +54,9 @@ constexpr int SP_XR = SP_TY + 4;      // x rows j0-2 .. j0+TY+1
 constexpr int SP_CR = SP_TY + 2;      // b, cx, cz rows j0-1 .. j0+TY
 constexpr int SP_YR = SP_TY + 3;      // cy rows j0-2 .. j0+TY
 constexpr int SP_NT = 320;            // 8 tile warps + ring rows + ring columns
+// the thread that issues the TMA copies and waits for them: lane 0 of the ring-column warp,
+// whose relaxation work per plane is the smallest
+constexpr int SP_PROD = SP_NT - 32;
 #ifndef MF3D_SP_D
 #define MF3D_SP_D 3 // planes staged ahead of the one the red stage reads
 #endif
@@ -178,6 +181,9 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TC, TM>()))
                   "FP64 or FP32 vectors with coefficients of the same type, or FP32 / BF16 with TMA staging");
     constexpr bool ZERO = (MODE & M_ZERO) != 0, PROL = (MODE & M_PROLONG) != 0, DOT = (MODE & M_DOT) != 0;
     static_assert((MODE & M_RESID) == 0, "the residual runs in a kernel of its own");
+    // the producer thread; FP64 prolongation sweeps keep it in tile warp 0 (measured faster
+    // there: 0.181 against 0.193 ms at 256^3, where the other sweeps gain 5-9% in warp 9)
+    constexpr int PROD = (PROL && sizeof(T) == 8) ? 0 : SP_PROD;
     using G = SpGeom<T, TC, TM>;
     constexpr int ST = G::ST, SC = G::SC, W = G::W, HX = G::HX, NP = G::NP, TX = G::TX;
     constexpr int QS = 32; // cells between the pairs of one lane (16 lanes x one pair each)
@@ -218,11 +224,11 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TC, TM>()))
     auto nxs = [](int s) { return s + 1 == SP_NSX ? 0 : s + 1; };
     auto ncs = [](int s) { return s + 1 == SP_NSC ? 0 : s + 1; };
     double dot_acc = 0.0;
-    // TMA form: thread 0 issues every copy and waits on the groups' barriers
-    unsigned phase = 0u; // thread 0: parity of the next wait, per barrier
+    // TMA form: the producer thread issues every copy and waits on the groups' barriers
+    unsigned phase = 0u; // producer: parity of the next wait, per barrier
     bool fail = false;
     if constexpr (TM) {
-        if (tid == 0) {
+        if (tid == PROD) {
             for (int k = 0; k < SP_NSX; ++k) mbar_init(&sp_full[k], 1);
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
@@ -249,7 +255,7 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TC, TM>()))
         if constexpr (TM) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads(); // the previous item's reads (and generic writes) of the slots are done
         if constexpr (BATCH) {
-            if (tid == 0) { // tensor maps read from global memory: order them before their use
+            if (tid == PROD) { // tensor maps read from global memory: order them before their use
                 const CUtensorMap* mp[8] = {&maps.x, &maps.b, &maps.cx, &maps.cy, &maps.cz, &maps.bxm, &maps.bym, &maps.bzm};
 #pragma unroll
                 for (int k = 0; k < 8; ++k)
@@ -286,17 +292,17 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TC, TM>()))
             return v;
         };
         int sxi = 0, sci = SP_NSC - 1; // slots of the next group's x plane and coefficient plane
-        int next_wait = P0;            // thread 0 (TMA form): the next group to wait for
+        int next_wait = P0;            // the producer (TMA form): the next group to wait for
         // slots of the planes the first step (t = z0 - 1) reads: x t-1, t, t+1; coefficients t
         int sxm = 0, sx0 = 1, sx1 = 2, sc0 = 1;
         auto advance = [&]() { // the issue slots advance as the groups are issued
             sxm = sx0, sx0 = sx1, sx1 = nxs(sx1);
             sc0 = ncs(sc0);
         };
-        // ---- TMA form: thread 0's copies of group p and its waits ----
+        // ---- TMA form: the producer's copies of group p and its waits ----
         auto tma_issue = [&](int p) {
             if constexpr (TM) {
-                if (tid == 0 && real(p)) {
+                if (tid == PROD && real(p)) {
                     const int q = p - 1;
                     const bool dox = !ZERO && p <= XL, doc = q >= P0 && q <= CL;
                     uint64_t* bar = &sp_full[sxi];
@@ -322,16 +328,16 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TC, TM>()))
                 }
             }
         };
-        // thread 0 waits for group p (x slot s); the barrier publishes it (and this step's red
+        // the producer waits for group p (x slot s); the barrier publishes it (and this step's red
         // values); false when a wait gave up
         auto sync_step = [&](int p, int s) -> bool {
             if constexpr (TM) {
                 bool bad = false;
-                if (tid == 0 && real(p)) {
+                if (tid == PROD && real(p)) {
                     bad = !mbar_wait(&sp_full[s], (phase >> s) & 1u);
                     if (!bad) phase ^= 1u << s;
                 }
-                if (tid == 0 && !bad) next_wait = p + 1;
+                if (tid == PROD && !bad) next_wait = p + 1;
                 // generic writes to the slots (red values, corrections) before later TMA writes
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 return !bar_red_or(1, SP_NT, bad);
@@ -345,7 +351,7 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TC, TM>()))
         auto sync_prologue = [&]() -> bool {
             if constexpr (TM) {
                 bool bad = false;
-                if (tid == 0) {
+                if (tid == PROD) {
                     for (int p = P0; p <= P0 + 1 && !bad; ++p) {
                         if (real(p)) {
                             const int s = p - P0;
@@ -363,11 +369,11 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TC, TM>()))
                 return true;
             }
         };
-        // after a failed wait: thread 0 waits (bounded) for the groups it issued and nobody
+        // after a failed wait: the producer waits (bounded) for the groups it issued and nobody
         // waited for yet, so that no copy is in flight when the CTA leaves
         auto drain = [&](int p_last) {
             if constexpr (TM) {
-                if (tid == 0) {
+                if (tid == PROD) {
                     atomicExch(a.err, 1);
                     for (int p = next_wait; p <= p_last; ++p) {
                         if (!real(p)) continue;
@@ -677,13 +683,16 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TC, TM>()))
                         }
                     }
                     asm volatile("cp.async.commit_group;" ::: "memory");
+                } else {
+                    tma_issue(p); // (the producer thread may be in this role)
                 }
-                sxi = nxs(sxi); // (TMA form: thread 0 stages everything)
+                sxi = nxs(sxi);
                 sci = ncs(sci);
             };
 #pragma unroll
             for (int q = 0; q <= SP_D; ++q) issue(P0 + q);
             if (!sync_prologue()) {
+                drain(P0 + SP_D);
                 fail = true;
                 break;
             }
@@ -705,6 +714,7 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TC, TM>()))
             }
             for (int t = z0 - 1; t <= z1; ++t) {
                 if (!sync_step(t + 1, sx1)) {
+                    drain(t + SP_D - 1);
                     fail = true;
                     break;
                 }
