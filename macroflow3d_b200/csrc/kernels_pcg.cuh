@@ -412,14 +412,45 @@ __device__ __forceinline__ void xr_update_body(size_t n, double* __restrict__ x,
     }
     const double alpha = s.rho_new / s.pAp;
     double srr = 0.0, sg = 0.0;
-    for (size_t c = blk * (size_t)PK_NT + threadIdx.x; c < n; c += (size_t)nblk * PK_NT) {
+    // two cells per thread and pass (16-byte loads and stores); the vectors come from whole
+    // allocations, so a pair starts on a 16-byte boundary; an odd last cell goes to thread 0
+    auto cell = [&](size_t c) {
         x[c] = x[c] + alpha * p[c];
         const double rv = r[c] + (-alpha) * Ap[c];
         r[c] = rv;
         if (r32) r32[c] = (float)rv;
         srr += rv * rv;
         if (s.flexible) sg += rv * (double)z[c];
+    };
+    const size_t n2 = n >> 1;
+    for (size_t c2 = blk * (size_t)PK_NT + threadIdx.x; c2 < n2; c2 += (size_t)nblk * PK_NT) {
+        double2 xv = reinterpret_cast<const double2*>(x)[c2];
+        const double2 pv = reinterpret_cast<const double2*>(p)[c2];
+        double2 rv = reinterpret_cast<const double2*>(r)[c2];
+        const double2 av = reinterpret_cast<const double2*>(Ap)[c2];
+        xv.x = xv.x + alpha * pv.x;
+        xv.y = xv.y + alpha * pv.y;
+        rv.x = rv.x + (-alpha) * av.x;
+        rv.y = rv.y + (-alpha) * av.y;
+        reinterpret_cast<double2*>(x)[c2] = xv;
+        reinterpret_cast<double2*>(r)[c2] = rv;
+        if (r32) reinterpret_cast<float2*>(r32)[c2] = make_float2((float)rv.x, (float)rv.y);
+        srr += rv.x * rv.x;
+        srr += rv.y * rv.y;
+        if (s.flexible) {
+            double z0, z1;
+            if constexpr (sizeof(TZ) == 8) {
+                const double2 zv = reinterpret_cast<const double2*>(z)[c2];
+                z0 = zv.x, z1 = zv.y;
+            } else {
+                const float2 zv = reinterpret_cast<const float2*>(z)[c2];
+                z0 = (double)zv.x, z1 = (double)zv.y;
+            }
+            sg += rv.x * z0;
+            sg += rv.y * z1;
+        }
     }
+    if ((n & 1) && blk == 0 && threadIdx.x == 0) cell(n - 1);
     double v[2] = {srr, sg}, out[2];
     if (grid_sums<PK_NT, 2>(v, partials, ticket, nblk, out, blk)) {
         const int it = s.iter + 1;
