@@ -224,7 +224,7 @@ typedef struct mf3d_batch mf3d_batch;
 typedef struct mf3d_batch_tuning {
     int phase;        /* 0 pre-smoothing (down), 1 post-smoothing (up) */
     int level;        /* level depth */
-    int sweep;        /* sweep index, 1-based */
+    int sweep;        /* 2 x the sweep index (1-based); + 1: the residual + restriction after it */
     int mode;         /* fused stages of the sweep (first-sweep zero guess 1, prolongation 2, residual+restriction 4, <r,z> 8) */
     int path;         /* 0 staged quad sweep where the level is 16-byte aligned, 1 L1 sweep for all,
                          2 x-pair sweep (TMA) where it serves, else as 0 */

@@ -79,8 +79,12 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
     using VC = VCycle<T, TC>;
     using Rec = typename VC::RecSweep;
 
-    // one batched launch of a sweep position: x-pair (TMA), staged quad (TMA) or L1 form
+    // one batched launch of a sweep position: x-pair (TMA), staged quad (TMA) or L1 form; or
+    // of a residual + restriction position
     struct Launch {
+        bool rr = false;
+        const RrItem<T, TC>* ritems = nullptr;
+        const int* roff = nullptr;
         bool pair = false;
         SpArgs<T, TC> pa0{}; // x-pair: the launch-wide argument
         bool tma = false;
@@ -118,6 +122,8 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
         occ_[M_ZERO | M_DOT] = tma_batch_setup<T, TC, M_ZERO | M_DOT>();
         occ_[M_PROLONG | M_DOT] = tma_batch_setup<T, TC, M_PROLONG | M_DOT>();
         occ_[M_ZERO | M_PROLONG | M_DOT] = tma_batch_setup<T, TC, M_ZERO | M_PROLONG | M_DOT>();
+        MF3D_CK(cudaFuncSetAttribute(resid_restrict_batch_kernel<T, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)rr_smem_bytes<T, TC>()));
         if constexpr (VC::kPair) {
             pocc_[0] = pair_batch_setup<T, TC, 0>();
             pocc_[M_ZERO] = pair_batch_setup<T, TC, M_ZERO>();
@@ -156,9 +162,12 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
             for (int r = 0; r < R; ++r)
                 for (const Rec& x : recs[r]) {
                     if (x.phase != phase) continue;
+                    // one launch per position and mode: a position's last pre-sweep is the fused
+                    // RESID sweep for some realisations and a sweep followed by its own residual +
+                    // restriction (sw + 1) for others
                     Op* op = nullptr;
                     for (Op& o : ops)
-                        if (o.level == x.level && o.sw == x.sw) op = &o;
+                        if (o.level == x.level && o.sw == x.sw && o.mode == x.mode) op = &o;
                     if (!op) {
                         ops.push_back(Op{});
                         op = &ops.back();
@@ -362,6 +371,13 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
             t.sweep = o.sw;
             t.mode = o.mode;
             t.ms_default = time_launches(o.mode, o.launches, reps);
+            if (o.rec[0].kind == 1) { // residual + restriction: one shape
+                t.path = o.path;
+                t.chunks = o.chunks;
+                t.ms_best = t.ms_default;
+                out.push_back(t);
+                continue;
+            }
             int best_path = o.path, best_chunks = o.chunks;
             double best = t.ms_default;
             bool any_tma = false, any_pair = false;
@@ -435,6 +451,32 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
     static constexpr int pair_tx() { return sp_tx<T, TC, true>(); }
 
     std::vector<Launch> build(const Op& o, int path, int chunks) const {
+        if (o.rec[0].kind == 1) { // residual + restriction of every realisation at this position
+            std::vector<int> off(1, 0);
+            std::vector<RrItem<T, TC>> items;
+            for (int i = 0; i < (int)o.rec.size(); ++i) {
+                RrItem<T, TC> it = o.rec[i].rr;
+                HeadSolver& H = *hs_[o.real[i]];
+                it.stop = &H.state_.as<PcgState>()->stop;
+                off.push_back(off.back() + it.gx * it.gy * it.gz);
+                items.push_back(it);
+            }
+            Blob b;
+            const size_t oo = b.add(off.data(), off.size() * sizeof(int));
+            const size_t oi = b.add(items.data(), items.size() * sizeof(items[0]));
+            Launch L;
+            L.rr = true;
+            L.nseg = (int)items.size();
+            L.total = off.back();
+            L.grid = (unsigned)L.total;
+            L.mem = b.upload();
+            unsigned char* base = L.mem->template as<unsigned char>();
+            L.roff = reinterpret_cast<const int*>(base + oo);
+            L.ritems = reinterpret_cast<const RrItem<T, TC>*>(base + oi);
+            std::vector<Launch> out;
+            out.push_back(std::move(L));
+            return out;
+        }
         std::vector<int> ps, ts, ls;
         for (int i = 0; i < (int)o.rec.size(); ++i) {
             const Rec& x = o.rec[i];
@@ -575,6 +617,11 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
     }
 
     void launch(cudaStream_t s, int mode, const Launch& L) const {
+        if (L.rr) {
+            resid_restrict_batch_kernel<T, TC><<<L.grid, 256, rr_smem_bytes<T, TC>(), s>>>(L.ritems, L.roff, L.nseg);
+            MF3D_LAUNCH_CK();
+            return;
+        }
         switch (mode) {
         case 0: launch_one<0>(s, L); break;
         case M_ZERO: launch_one<M_ZERO>(s, L); break;

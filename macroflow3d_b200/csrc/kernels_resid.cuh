@@ -53,10 +53,11 @@ template <class T, class E> __device__ __forceinline__ void rr_pair(const E* p, 
     b = rr_one<T>(p + 1);
 }
 
+// One CTA's work: tile (bx, by) of 32 x 16 cells, z chunk bz.
 template <class T, class TC>
-__global__ void __launch_bounds__(256, MF3D_RR_MINB)
-    resid_restrict_staged_kernel(const LevelOp<TC> L, const T* __restrict__ x, const T* __restrict__ b,
-                                 T* __restrict__ b_coarse, int zchunk) {
+__device__ __forceinline__ void resid_restrict_body(const LevelOp<TC>& L, const T* __restrict__ x,
+                                                    const T* __restrict__ b, T* __restrict__ b_coarse, int zchunk,
+                                                    int bx, int by, int bz) {
     // cp.async moves 4, 8 or 16 bytes per copy: a pair of BF16 faces is one 4-byte copy, and the
     // single -x face of a row (kind 3 below) is loaded one plane ahead and stored by hand
     static_assert(sizeof(T) >= 4 && (sizeof(TC) >= 4 || std::is_same<TC, __nv_bfloat16>::value),
@@ -69,8 +70,8 @@ __global__ void __launch_bounds__(256, MF3D_RR_MINB)
     const int tx = lane & 15, ty = 2 * warp + (lane >> 4); // pair tx of row ty
     const int nx = L.nx, ny = L.ny, nz = L.nz, ncx = nx >> 1, ncy = ny >> 1;
     const size_t nxy = (size_t)nx * ny;
-    const int i0 = blockIdx.x * RR_TX, j0 = blockIdx.y * RR_TY, i = i0 + 2 * tx, j = j0 + ty;
-    const int k0 = blockIdx.z * zchunk, k1 = min(k0 + zchunk, nz);
+    const int i0 = bx * RR_TX, j0 = by * RR_TY, i = i0 + 2 * tx, j = j0 + ty;
+    const int k0 = bz * zchunk, k1 = min(k0 + zchunk, nz);
     const bool own = i < nx && j < ny; // both cells of the pair (nx even)
     const T inv_dx2 = (T)L.inv_dx2;
     auto xy_of = [&](int ii, int jj, long long& g) {
@@ -219,6 +220,35 @@ __global__ void __launch_bounds__(256, MF3D_RR_MINB)
         czm0 = czp0, czm1 = czp1;
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+template <class T, class TC>
+__global__ void __launch_bounds__(256, MF3D_RR_MINB)
+    resid_restrict_staged_kernel(const LevelOp<TC> L, const T* __restrict__ x, const T* __restrict__ b,
+                                 T* __restrict__ b_coarse, int zchunk) {
+    resid_restrict_body<T, TC>(L, x, b, b_coarse, zchunk, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// The residual + restriction of several realisations in one launch: realisation s owns the
+// CTAs [off[s], off[s+1]) (its gx x gy x gz grid); realisations whose solve has stopped are
+// skipped.
+template <class T, class TC> struct RrItem {
+    LevelOp<TC> L;
+    const T* x;
+    const T* b;
+    T* out;
+    int zchunk, gx, gy, gz;
+    const int* stop;
+};
+template <class T, class TC>
+__global__ void __launch_bounds__(256, MF3D_RR_MINB)
+    resid_restrict_batch_kernel(const RrItem<T, TC>* __restrict__ items, const int* __restrict__ off, int nseg) {
+    const int s = find_seg(off, nseg, blockIdx.x);
+    const RrItem<T, TC>& it = items[s];
+    if (it.stop && *it.stop) return; // that realisation's solve has finished (CTA-uniform)
+    const int v = blockIdx.x - __ldg(off + s);
+    resid_restrict_body<T, TC>(it.L, it.x, it.b, it.out, it.zchunk, v % it.gx, (v / it.gx) % it.gy,
+                               v / (it.gx * it.gy));
 }
 
 } // namespace mf3d

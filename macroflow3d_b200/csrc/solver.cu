@@ -763,6 +763,8 @@ template <class T, class TC> class VCycle : public VCycleBase {
         bool pair;            // the x-pair sweep's TMA form serves this sweep
         SpArgs<T, TC> pa;     // its arguments, z chunk unset
         const SpMaps* pmaps;  // its tensor maps
+        int kind;             // 0: a sweep; 1: the residual + restriction after the last pre-sweep
+        RrItem<T, TC> rr;     // kind 1: its arguments and grid
     };
     struct RecTail {
         Tail2Args a;
@@ -815,10 +817,12 @@ template <class T, class TC> class VCycle : public VCycleBase {
                 T* out = other(l, c);
                 int mode = (c ? 0 : M_ZERO) | (sw == pre_ ? M_RESID : 0);
                 rec_phase_ = 0;
-                rec_sw_ = sw;
+                rec_sw_ = 2 * sw; // (2 sw + 1: the residual + restriction after it)
                 // staged levels: the last pre-sweep, then the residual and its restriction in a
-                // kernel of their own (batched solves keep the fused form they record)
-                const bool split = (mode & M_RESID) && (tma_[l] || pair_[l]) && split_resid_ && !rec_;
+                // kernel of their own (batched solves record it so where the x-pair sweep serves,
+                // else the fused form)
+                const bool split = (mode & M_RESID) && (tma_[l] || pair_[l]) && split_resid_ &&
+                                   (!rec_ || (pair_[l] && pair_tm_[l]));
                 sweep(s, l, c, out, nullptr, split ? nullptr : bc_next, split ? (mode & ~M_RESID) : mode, nullptr);
                 if (split) resid_restrict(s, l, out, bc_next);
                 c = out;
@@ -843,7 +847,7 @@ template <class T, class TC> class VCycle : public VCycleBase {
                 T* out = (l == 0 && last) ? z : other(l, c);
                 int mode = (c ? 0 : M_ZERO) | (sw == 1 ? M_PROLONG : 0) | ((l == 0 && last && rho_out) ? M_DOT : 0);
                 rec_phase_ = 1;
-                rec_sw_ = sw;
+                rec_sw_ = 2 * sw; // (2 sw + 1: the residual + restriction after it)
                 sweep(s, l, c, out, e, nullptr, mode, rho_out);
                 c = out;
             }
@@ -1035,6 +1039,7 @@ template <class T, class TC> class VCycle : public VCycleBase {
             r.la = ldg_args(l, x_in, x_out, e, b_coarse, dot_out);
             r.pair = false;
             r.pmaps = nullptr;
+            r.kind = 0;
             if constexpr (kPair) {
                 if (pair_[l] && pair_tm_[l] && !(mode & M_RESID)) {
                     r.pair = true;
@@ -1213,6 +1218,25 @@ template <class T, class TC> class VCycle : public VCycleBase {
                 1, std::min<long long>(ncz, (long long)num_sms() * MF3D_RR_PERSM / std::max(1LL, tiles)));
             const int zc = 2 * ((ncz + nzc - 1) / nzc);
             const dim3 grid(gx, gy, (g.nz + zc - 1) / zc);
+            if (rec_) { // batched solve: record only
+                RecSweep r{};
+                r.phase = rec_phase_;
+                r.level = l;
+                r.sw = rec_sw_ + 1;
+                r.mode = -1;
+                r.g = g;
+                r.kind = 1;
+                r.rr.L = ops_[l];
+                r.rr.x = x;
+                r.rr.b = b;
+                r.rr.out = out;
+                r.rr.zchunk = zc;
+                r.rr.gx = (int)grid.x;
+                r.rr.gy = (int)grid.y;
+                r.rr.gz = (int)grid.z;
+                rec_->push_back(r);
+                return;
+            }
             MF3D_CK(cudaFuncSetAttribute(resid_restrict_staged_kernel<T, TC>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rr_smem_bytes<T, TC>()));
             resid_restrict_staged_kernel<T, TC><<<grid, 256, rr_smem_bytes<T, TC>(), s>>>(ops_[l], x, b, out, zc);
