@@ -30,6 +30,35 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 HBM_FALLBACK_GBS = 6650.0
+T0 = time.perf_counter()
+
+
+def note(msg):
+    """Progress on stderr (stdout carries only the JSON line)."""
+    print(f"[bench {time.perf_counter() - T0:7.1f} s] {msg}", file=sys.stderr, flush=True)
+
+
+def host_cores():
+    """Cores this process may use: the CPU affinity mask, capped by a cgroup CPU quota (a
+    container can see every core of the host but be allowed only a few; OpenMP with one thread
+    per visible core then oversubscribes the allowed ones)."""
+    n = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    quota = None
+    try:
+        q, per = open("/sys/fs/cgroup/cpu.max").read().split()[:2]
+        if q != "max":
+            quota = int(q) / int(per)
+    except (OSError, ValueError):
+        try:
+            q = int(open("/sys/fs/cgroup/cpu/cpu.cfs_quota_us").read())
+            per = int(open("/sys/fs/cgroup/cpu/cpu.cfs_period_us").read())
+            if q > 0 and per > 0:
+                quota = q / per
+        except (OSError, ValueError):
+            pass
+    if quota is not None:
+        n = min(n, max(1, int(quota)))
+    return max(1, n)
 
 
 def peaks():
@@ -267,6 +296,7 @@ def warmstart_eval(M, precision, seed):
         g = M.Grid3D(n, n, n, 1.0)
         s = M.HeadSolver(g, bc, solver_cfg(M, n, precision), stream=stream.cuda_stream)
         for k, (s2, lam) in enumerate([(1.0, 6.0), (2.5, 8.0), (4.0, 10.0)]):
+            note(f"held-out field {n}^3, sigma2 {s2:g}, lambda {lam:g}")
             K = M.generate_K_field(g, s2, (lam, lam, lam), seed=seed + 9_000_000 + 100 * n + k, n_modes=1000)
             s.set_K(K)
             h = torch.empty_like(K)
@@ -396,6 +426,7 @@ def _ensemble_arms(M, b, solvers, grids, shapes, bc, cfg, Ks, hs, velocities, ti
     stream = torch.cuda.current_stream()
     b.set_K(Ks)
     tuning = b.autotune(tune_reps) if tune_reps > 0 else []
+    note(f"ensemble: autotuned {len(tuning)} positions; batched steps")
 
     def bstep():
         b.set_K(Ks)
@@ -404,6 +435,7 @@ def _ensemble_arms(M, b, solvers, grids, shapes, bc, cfg, Ks, hs, velocities, ti
         return r
 
     ms_b, res_b = timed(bstep)
+    note("ensemble: looped single solves")
     h_batch = [h.clone() for h in hs[:4]]
     # ---- looping single solves ----
     for g, sh in zip(grids, shapes):
@@ -456,7 +488,7 @@ def cpu_baseline(K_np, n, budget_s=60.0, reps=3):
     of `reps` FULL solves (set-up + PCG to ||r||/||b|| <= 1e-10 + one velocity pass) of the
     same workload; fewer when one solve alone takes more than a third of `budget_s`."""
     from oracle import oracle as O
-    cores = os.cpu_count() or 1
+    cores = host_cores()
     O.set_threads(cores)
     bc = O.baseline_bc()
     lv = levels_for(n)
@@ -468,6 +500,7 @@ def cpu_baseline(K_np, n, budget_s=60.0, reps=3):
         h, res = O.solve_head_pcg(K_np, bc, lv, max_iter=500, check_every=1, rtol=rtol)
         O.velocity(h, K_np, bc)
         times.append(time.perf_counter() - t)
+        note(f"oracle solve {len(times)}: {times[-1]:.2f} s, {res.iterations} iterations")
         iters = res.iterations
         if time.perf_counter() - t_all > budget_s * (len(times) + 1) / (reps + 1):
             break
@@ -585,6 +618,7 @@ def main():
     K = make_K(M, n, sigma2, lam, replica_seed(args.seed, rank), torch.cuda.current_device())
     torch.cuda.synchronize()
 
+    note(f"{n}^3 {args.precision}: {args.warmup} warm-up + {args.steps} timed steps")
     with Clocks(torch.cuda.current_device()) as clk:
         out = run_steps(M, n, K, prec, args.steps, args.warmup, dist_ctx)
     clocks = clk.summary()
@@ -613,6 +647,7 @@ def main():
     out["solver"].close()
 
     if not args.no_fp64_compare and prec != M.PREC_FP64:
+        note("plain FP64 solver on the same field")
         o64 = run_steps(M, n, K, M.PREC_FP64, args.steps, args.warmup, dist_ctx)
         ms64 = o64["ms_total"]
         line["fp64_plain"] = {"solves_per_s": round(world * args.steps / (ms64 / 1e3), 4),
@@ -627,6 +662,7 @@ def main():
         iters64 = out["iters"][-1]
 
     if rank == 0 and world == 1 and not args.no_e2e:
+        note("end to end through host buffers")
         K_host = K.cpu().pin_memory()
         v, bi, bo = e2e_steps(M, n, K_host, prec, max(4, args.steps), 2)
         line["e2e"] = {"value": round(v, 4), "unit": "solves/s", "h2d_bytes_per_step": bi,
@@ -634,8 +670,10 @@ def main():
                        "copies": "second stream, double-buffered: the next K up and the previous head "
                                  "down while a step solves"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        note(f"CPU baseline on {host_cores()} cores")
         line["cpu_baseline"] = cpu_baseline(K.cpu().numpy(), n)
     if rank == 0 and world == 1 and not args.no_learned:
+        note("learned initial guess")
         ws = M.WarmStart.pretrained()
         ol = run_steps(M, n, K, prec, args.steps, args.warmup, None, warmstart=ws)
         v_l = args.steps / (ol["ms_total"] / 1e3)
@@ -647,10 +685,12 @@ def main():
                                  "speedup_vs_mixed": round(v_l / value, 3)}
         ol["solver"].close()
         ws.close()
+        note("learned initial guess on held-out fields")
         line["warm_start_c5"] = warmstart_eval(M, prec, args.seed)
     if rank == 0 and world == 1 and not args.no_ensemble:
         del K
         torch.cuda.empty_cache()
+        note(f"ensemble of {args.ensemble_count} realisations")
         line["ensemble"] = ensemble_steps(M, prec, args.ensemble_count, 3, 3, args.seed)
 
     if rank == 0:
@@ -670,7 +710,7 @@ def reference_arm(args, n, sigma2, lam, config):
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded randomization-method lnK field)", "config": config}
-    O.set_threads(os.cpu_count() or 1)
+    O.set_threads(host_cores())
     lams = tuple(lam) if isinstance(lam, (tuple, list)) else (lam, lam, lam)
     K = O.generate_K((n, n, n), sigma2, lams, seed=args.seed, n_modes=1000)
     bc = O.baseline_bc()

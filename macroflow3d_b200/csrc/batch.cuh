@@ -392,6 +392,7 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
                     if (path == o.path && chunks == o.chunks) continue;
                     std::vector<Launch> cand = build(o, path, chunks);
                     const double ms = time_launches(o.mode, cand, reps);
+                    retire(cand);
                     if (ms < best) {
                         best = ms;
                         best_path = path;
@@ -401,6 +402,7 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
             if (best_path != o.path || best_chunks != o.chunks) {
                 o.path = best_path;
                 o.chunks = best_chunks;
+                retire(o.launches);
                 o.launches = build(o, o.path, o.chunks);
             }
             t.path = o.path;
@@ -599,6 +601,15 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
 
     VC* vc_of(int r) const { return static_cast<VC*>(hs_[r]->vc_.get()); }
 
+    // Launch tables hold tensor maps that kernels read from device memory.  A table is never
+    // freed while the solver lives, so no later table (another candidate's maps) is written
+    // at an address whose descriptor the TMA unit may still cache.
+    void retire(std::vector<Launch>& ls) {
+        for (Launch& L : ls)
+            if (L.mem) retired_.push_back(std::move(L.mem));
+        ls.clear();
+    }
+
     template <int MODE> void launch_one(cudaStream_t s, const Launch& L) const {
         if (L.pair) {
             if constexpr (VC::kPair && (MODE & M_RESID) == 0) {
@@ -769,6 +780,7 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
     int occ_[16] = {};
     int pocc_[16] = {}; // resident batched x-pair-sweep CTAs per SM, by mode
     std::vector<Op> ops_;
+    std::vector<std::unique_ptr<DevMem>> retired_; // launch tables of candidates no longer used
     std::unique_ptr<DevMem> tail_mem_, pcg_mem_;
     size_t tail_smem_ = 0;
     PcgItem* items_d_ = nullptr;

@@ -255,11 +255,14 @@ __global__ void __launch_bounds__(SP_NT, (sp_minb<T, TC, TM>()))
         if constexpr (TM) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads(); // the previous item's reads (and generic writes) of the slots are done
         if constexpr (BATCH) {
-            if (tid == PROD) { // tensor maps read from global memory: order them before their use
+            if (tid == PROD) {
+                // tensor maps read from global memory, written there by a host copy: the acquire
+                // has system scope (a narrower scope may leave the TMA unit a stale descriptor
+                // cached for the same address)
                 const CUtensorMap* mp[8] = {&maps.x, &maps.b, &maps.cx, &maps.cy, &maps.cz, &maps.bxm, &maps.bym, &maps.bzm};
 #pragma unroll
                 for (int k = 0; k < 8; ++k)
-                    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(mp[k]) : "memory");
+                    asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(mp[k]) : "memory");
             }
         }
         const int tile = item % ntiles;

@@ -399,12 +399,14 @@ __global__ void __launch_bounds__(TmaSweepCfg<T, TC, MODE>::NT, TmaSweepCfg<T, T
             // coefficient plane p), each copy into a slot the consumers have released ----
             if (tid == C::NCONS) {
                 if constexpr (BATCH) {
-                    // tensor maps read from global memory: order them before their use by TMA
+                    // tensor maps read from global memory, written there by a host copy: the
+                    // acquire has system scope (a narrower scope may leave the TMA unit a stale
+                    // descriptor cached for the same address)
                     const CUtensorMap* mp[8] = {&maps.x, &maps.b, &maps.cx, &maps.cy, &maps.cz,
                                                 &maps.bxm, &maps.bym, &maps.bzm};
 #pragma unroll
                     for (int k = 0; k < 8; ++k)
-                        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(mp[k]) : "memory");
+                        asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(mp[k]) : "memory");
                 }
                 auto issue_x = [&](int p) {
                     const unsigned n = qx + (unsigned)(p - pl0);
