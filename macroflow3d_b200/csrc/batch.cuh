@@ -283,6 +283,7 @@ template <class T, class TC> class BatchSolverT : public BatchSolverBase {
         for (const auto& h : hs_) b += h->device_bytes();
         for (const Op& o : ops_)
             for (const Launch& l : o.launches) b += (long long)l.mem->bytes;
+        for (const auto& m : retired_) b += (long long)m->bytes;
         return b + (long long)tail_mem_->bytes + (long long)pcg_mem_->bytes;
     }
 
