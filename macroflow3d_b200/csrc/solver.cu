@@ -819,10 +819,8 @@ template <class T, class TC> class VCycle : public VCycleBase {
                 rec_phase_ = 0;
                 rec_sw_ = 2 * sw; // (2 sw + 1: the residual + restriction after it)
                 // staged levels: the last pre-sweep, then the residual and its restriction in a
-                // kernel of their own (batched solves record it so where the x-pair sweep serves,
-                // else the fused form)
-                const bool split = (mode & M_RESID) && (tma_[l] || pair_[l]) && split_resid_ &&
-                                   (!rec_ || (pair_[l] && pair_tm_[l]));
+                // kernel of their own (batched solves record the fused form)
+                const bool split = (mode & M_RESID) && (tma_[l] || pair_[l]) && split_resid_ && !rec_;
                 sweep(s, l, c, out, nullptr, split ? nullptr : bc_next, split ? (mode & ~M_RESID) : mode, nullptr);
                 if (split) resid_restrict(s, l, out, bc_next);
                 c = out;

@@ -145,7 +145,7 @@ def test_autotune_keeps_results(mf3d):
     b0, base, _ = _batch(M, grids, bc, cfg, Ks)
     b1, tuned, tuning = _batch(M, grids, bc, cfg, Ks, tune=True)
     assert tuning and all(t["ms_best"] <= t["ms_default"] + 1e-9 for t in tuning)
-    assert {t["path"] for t in tuning} <= {0, 1, 2}  # quad, L1, x-pair
+    assert {t["path"] for t in tuning} <= {0, 1}  # quad, L1 (the batched x-pair sweep is off)
     for (h0, r0), (h1, r1) in zip(base, tuned):
         assert r1.converged and abs(r1.num_iterations - r0.num_iterations) <= 1
         assert _rel(h1, h0) < HEAD_TOL
