@@ -226,8 +226,8 @@ typedef struct mf3d_batch_tuning {
     int level;        /* level depth */
     int sweep;        /* 2 x the sweep index (1-based); + 1: the residual + restriction after it */
     int mode;         /* fused stages of the sweep (first-sweep zero guess 1, prolongation 2, residual+restriction 4, <r,z> 8) */
-    int path;         /* 0 staged quad sweep where the level is 16-byte aligned, 1 L1 sweep for all,
-                         2 x-pair sweep (TMA) where it serves, else as 0 */
+    int path;         /* 0 staged quad sweep where the level is 16-byte aligned, 1 L1 sweep for all
+                         (2, the batched x-pair sweep, is currently not chosen) */
     int chunks;       /* z chunks per tile: the z depth of a work item is nz / chunks */
     double ms_default;/* device time of the default choice */
     double ms_best;   /* device time of the choice kept */
