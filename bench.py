@@ -364,6 +364,29 @@ def warmstart_eval(M, precision, seed):
 ENSEMBLE_EDGES = (64, 96, 128, 160)
 
 
+ENSEMBLE_TIMEOUT_S = 240
+
+
+def ensemble_isolated(cmd, timeout_s):
+    """The ensemble record from `cmd` (bench.py --ensemble-only) run as a child process with
+    its own CUDA context and a time limit, so that the headline record does not depend on it:
+    a child that fails or runs out of time gives {"unavailable": why} instead.  The child's
+    progress lines are passed on to stderr."""
+    try:
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": f"the ensemble run exceeded {timeout_s} s"}
+    for ln in (p.stderr or "").splitlines()[-8:]:
+        print(ln, file=sys.stderr, flush=True)
+    if p.returncode != 0:
+        tail = (p.stderr or "").strip().splitlines()
+        return {"unavailable": f"the ensemble run exited {p.returncode}: {tail[-1] if tail else ''}"[:300]}
+    try:
+        return json.loads(p.stdout.strip().splitlines()[-1])["ensemble"]
+    except (ValueError, KeyError, IndexError):
+        return {"unavailable": "the ensemble run printed no record"}
+
+
 def ensemble_shapes(seed, count):
     """Grid edges drawn uniformly from ENSEMBLE_EDGES per axis and realisation (uneven sizes)."""
     import numpy as np
@@ -693,8 +716,11 @@ def main():
     if rank == 0 and world == 1 and not args.no_ensemble:
         del K
         torch.cuda.empty_cache()
-        note(f"ensemble of {args.ensemble_count} realisations")
-        line["ensemble"] = ensemble_steps(M, prec, args.ensemble_count, 3, 3, args.seed)
+        note(f"ensemble of {args.ensemble_count} realisations (child process)")
+        cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--ensemble-only", "--steps", "3", "--warmup", "3",
+               "--seed", str(args.seed), "--ensemble-count", str(args.ensemble_count),
+               "--precision", args.precision] + (["--no-graph"] if args.no_graph else [])
+        line["ensemble"] = ensemble_isolated(cmd, ENSEMBLE_TIMEOUT_S)
 
     if rank == 0:
         print(json.dumps(line), flush=True)
